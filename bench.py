@@ -1,0 +1,397 @@
+"""Benchmark: QPS at recall@10 >= 0.95 on 1M x 128, reduced precision + rerank vs FP32 plain.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (configuration 2 of the reference benchmark plan): 1,000,000 base
+vectors x 128 dims, integer-valued FP32 from a clipped 1,000-cluster Gaussian
+mixture (seeded, synthetic: no dataset is read), 10,000 queries; the index is
+built on the GPU with R=64, L=100, alpha=1.2 in batched inserts of 10,000.
+Ground truth is FP64 brute force.  Search L is swept; each form's operating
+point is the smallest L whose recall@10 >= 0.95.
+
+A step is one batched search of the 10,000 queries.  `value` is the headline
+form's (reduced-precision traversal + exact FP32 rerank) queries/s, device time
+with CUDA events on the launching stream, L2 flushed before every step.
+`e2e` repeats it through the public C ABI with pinned host buffers: each step
+copies the queries in and the ids/distances out inside the timed region.
+
+Multi-GPU: replicas only -- every rank builds the same index and searches its
+own full query batch; value = all ranks' queries / max-over-ranks time.
+--impl reference times the oracle's restatement of the reference's search
+(C, all host threads) on a bounded sample of the same queries over the same
+graph (built untimed on the GPU, as the reference's CPU path cannot build a
+1M graph within minutes).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cs5013-project_b200"))
+sys.path.insert(0, ROOT)
+
+N_BASE, N_QUERY, DIM, R, L_BUILD, ALPHA, BATCH, K = 1_000_000, 10_000, 128, 64, 100, 1.2, 10_000, 10
+L_SWEEP = [32, 40, 48, 56, 64, 80, 96, 128, 160, 192, 256]
+TARGET = 0.95
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_BASE)
+    ap.add_argument("--nq", type=int, default=N_QUERY)
+    ap.add_argument("--cpu-sample", type=int, default=2000)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="short run for a profiler capture")
+    return ap.parse_args()
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def ground_truth(torch, base_d, q_d, k):
+    """FP64 brute-force kNN on the GPU (exact for integer-valued data)."""
+    b64 = base_d.double()
+    bn = (b64 * b64).sum(1)
+    out = []
+    for s in range(0, q_d.shape[0], 512):
+        qq = q_d[s:s + 512].double()
+        d = (qq * qq).sum(1, keepdim=True) + bn[None, :] - 2.0 * qq @ b64.T
+        out.append(torch.topk(d, k, dim=1, largest=False).indices)
+    del b64
+    return torch.cat(out).int()
+
+
+def recall(torch, ids, gt, k=K):
+    a = ids[:, :k].long()
+    g = gt[:, :k].long()
+    hit = (a[:, :, None] == g[:, None, :]).any(2).sum().item()
+    return hit / (g.shape[0] * k)
+
+
+def build_index(torch, vann, base_d, dev):
+    idx = vann.Index(DIM, R, L_BUILD, ALPHA, capacity=base_d.shape[0], stores=("f32", "bf16", "fp8", "u8"))
+    torch.cuda.synchronize()
+    t0 = time.time()
+    idx.build(base_d, batch=BATCH, seed=2024)
+    torch.cuda.synchronize()
+    return idx, time.time() - t0
+
+
+def time_steps(torch, fn, steps, warmup, flush):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    times = []
+    for _ in range(steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times
+
+
+def main():
+    args = parse()
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference" and rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1 and args.impl == "ours":
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    import vann
+    from vann import workload
+
+    n, nq = args.n, args.nq
+    clusters = 1000 if n >= 100_000 else max(10, n // 1000)
+    base = workload.mixture(n, DIM, clusters, seed=1)
+    q = workload.mixture(nq, DIM, clusters, seed=2)
+    base_d = torch.from_numpy(base).to(dev)
+    q_d = torch.from_numpy(q).to(dev)
+    idx, build_s = build_index(torch, vann, base_d, dev)
+    gt = ground_truth(torch, base_d, q_d, K)
+
+    # ---- sweep
+    sweep = {}
+    forms = [("f32", False), ("bf16", False), ("u8", False), ("fp8", True)]
+    for store, rr in forms:
+        name = store + ("+rerank" if rr else "")
+        for L in L_SWEEP:
+            ids, _ = idx.search(q_d, k=K, L=L, store=store, rerank=rr)
+            torch.cuda.synchronize()
+            sweep.setdefault(name, []).append((L, recall(torch, ids, gt)))
+    idx.sync()
+
+    def op_point(name):
+        for L, r in sweep[name]:
+            if r >= TARGET:
+                return L, r
+        return sweep[name][-1]
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+    out = (torch.empty((nq, K), dtype=torch.int32, device=dev), torch.empty((nq, K), dtype=torch.float32, device=dev))
+    results = {}
+    steps, warm = (3, 1) if args.profile else (args.steps, args.warmup)
+    with Clocks(local) as clk:
+        for store, rr in forms:
+            name = store + ("+rerank" if rr else "")
+            L, r = op_point(name)
+            fn = lambda s=store, rr=rr, L=L: idx.search(q_d, k=K, L=L, store=s, rerank=rr, out=out)
+            t = time_steps(torch, fn, steps, warm, flush)
+            results[name] = {"L": L, "recall": r, "ms": t}
+    clocks = clk.summary()
+
+    # headline = fastest reduced-precision form at recall >= 0.95
+    def qps(name):
+        return nq / (statistics.mean(results[name]["ms"]) / 1e3)
+
+    reduced = [nm for nm in results if nm != "f32" and results[nm]["recall"] >= TARGET]
+    head = max(reduced, key=qps) if reduced else "f32"
+    hr = results[head]
+    mean_ms = statistics.mean(hr["ms"])
+    p50 = float(np.percentile(hr["ms"], 50))
+    p99 = float(np.percentile(hr["ms"], 99))
+
+    # work counters of the headline and FP32 forms (algorithmic bytes)
+    def counted_bytes(name):
+        store = name.split("+")[0]
+        rr = name.endswith("+rerank")
+        _, _, st = idx.search_stats(q_d, k=K, L=results[name]["L"], store=store, rerank=rr)
+        st = st.cpu().numpy().astype(np.int64)
+        hops, evals, adjw = st[0], st[1], st[2]
+        s = {"f32": 4, "bf16": 2, "u8": 1, "fp8": 1}[store]
+        sc = 4 if store == "fp8" else 0
+        L = results[name]["L"]
+        per_q = (hops * 4 + adjw * 4 + evals * (DIM * s + sc) + 4 * DIM + 8 * K
+                 + (min(L, 1 << 30) * 4 * DIM if rr else 0))
+        return float(per_q.sum()), float(hops.mean()), float(evals.mean())
+
+    bytes_head, hops_head, evals_head = counted_bytes(head)
+    bytes_f32, hops_f32, evals_f32 = counted_bytes("f32")
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = bytes_head / (mean_ms / 1e3) / 1e9
+
+    # ---- e2e through the public API with pinned host buffers
+    h_q = torch.from_numpy(q).pin_memory()
+    h_ids = torch.empty((nq, K), dtype=torch.int32).pin_memory()
+    h_d = torch.empty((nq, K), dtype=torch.float32).pin_memory()
+    q_tmp = torch.empty_like(q_d)
+    hs = head.split("+")[0]
+    hrr = head.endswith("+rerank")
+
+    def e2e_step():
+        q_tmp.copy_(h_q, non_blocking=True)
+        idx.search(q_tmp, k=K, L=hr["L"], store=hs, rerank=hrr, out=out)
+        h_ids.copy_(out[0], non_blocking=True)
+        h_d.copy_(out[1], non_blocking=True)
+
+    e2e_ms = time_steps(torch, e2e_step, steps, warm, flush)
+    e2e_qps = nq / (statistics.mean(e2e_ms) / 1e3)
+
+    # ---- max over ranks
+    total_s = sum(hr["ms"]) / 1e3
+    if dist is not None:
+        t = torch.tensor([total_s, sum(e2e_ms) / 1e3], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_s, e2e_total = t.tolist()
+        e2e_qps = world * nq * steps / e2e_total
+        dist.barrier()
+    value = world * nq * steps / total_s
+
+    # ---- CPU baseline: the oracle's search (same semantics as the FP32 form)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(idx, q, results["f32"]["L"], args.cpu_sample, hops_f32)
+
+    if rank == 0:
+        line = {
+            "metric": "QPS at recall@10>=0.95 (1Mx128), reduced-prec+rerank vs FP32 plain; p99 latency",
+            "value": round(value, 1), "unit": "queries/s", "n_gpus": world, "steps": steps, "warmup": warm,
+            "ms_per_step": round(mean_ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": {"f32": "f32", "bf16": "bf16", "u8": "u8", "fp8": "fp8e4m3"}[hs],
+            "data": "synthetic (seeded clipped Gaussian mixture)",
+            "config": {"workload": f"{n}x{DIM} integer-valued f32, 1000-cluster mixture; {nq} queries; "
+                                   f"build R={R} L={L_BUILD} alpha={ALPHA} batches of {BATCH}; k={K}",
+                       "headline_form": head, "L": hr["L"], "recall@10": round(hr["recall"], 4),
+                       "l2": "flushed before every step (256 MB write)", "parallelism": f"replicas x{world}",
+                       "build_s": round(build_s, 2)},
+            "p50_ms": round(p50, 4), "p99_ms": round(p99, 4),
+            "forms": {nm: {"L": v["L"], "recall@10": round(v["recall"], 4), "qps": round(qps(nm), 1),
+                           "p99_ms": round(float(np.percentile(v["ms"], 99)), 4)} for nm, v in results.items()},
+            "speedup_vs_fp32_plain": round(qps(head) / qps("f32"), 3),
+            "sweep": {nm: [[L, round(r, 4)] for L, r in v] for nm, v in sweep.items()},
+            "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": nq * DIM * 4,
+                    "d2h_bytes_per_step": nq * K * 8},
+            "gpu_launches": steps,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "algorithmic_bytes_per_launch": bytes_head, "hops_per_query": round(hops_head, 2),
+                         "evals_per_query": round(evals_head, 1), "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)"},
+            "clocks": clocks,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def cpu_baseline(idx, q, L, sample, hops_f32):
+    """Times the oracle port of the reference search over a bounded query sample."""
+    from oracle import oracle as O
+
+    O.build()
+    vecs, deg, adj = idx.get_graph()
+    g = O.Graph(vecs, deg, adj)
+    entry = idx.info()["entry"]
+    threads = os.cpu_count() or 1
+    qs = q[:sample]
+    t0 = time.time()
+    st, ids, d, hops, evals = g.search(qs, L, K, entry, threads=threads)
+    dt = time.time() - t0
+    return {"value": round(len(qs) / dt, 1), "unit": "queries/s", "cores": threads, "kind": "port",
+            "sample": f"{len(qs)} of the queries at L={L} (FP32), oracle/vann_oracle.c search, "
+                      f"{threads} threads; mean hops {hops.mean():.2f} (GPU counted {hops_f32:.2f})"}
+
+
+def main_reference():
+    """--impl reference: the oracle's search on all host cores, same config/metric."""
+    args = parse()
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import vann
+    from vann import workload
+    from oracle import oracle as O
+
+    O.build()
+    n, nq = args.n, args.nq
+    clusters = 1000 if n >= 100_000 else max(10, n // 1000)
+    base = workload.mixture(n, DIM, clusters, seed=1)
+    q = workload.mixture(nq, DIM, clusters, seed=2)
+    dev = torch.device("cuda", 0)
+    base_d = torch.from_numpy(base).to(dev)
+    idx, build_s = build_index(torch, vann, base_d, dev)
+    vecs, deg, adj = idx.get_graph()
+    entry = idx.info()["entry"]
+    del idx
+    torch.cuda.empty_cache()
+    g = O.Graph(vecs, deg, adj)
+    threads = os.cpu_count() or 1
+    # the FP32 operating point: smallest swept L with recall >= 0.95 on the sample
+    sample = args.cpu_sample
+    qs = q[:sample]
+    truth, _ = O.bruteforce_knn(base, qs[:200], K, threads=threads)
+    L_op = L_SWEEP[-1]
+    for L in L_SWEEP:
+        _, ids, _, _, _ = g.search(qs[:200], L, K, entry, threads=threads)
+        if O.recall_at_k(ids, truth, K) >= TARGET:
+            L_op = L
+            break
+    for _ in range(args.warmup):
+        g.search(qs[:200], L_op, K, entry, threads=threads)
+    times = []
+    for s in range(args.steps):
+        sub = q[(s * sample) % nq:][:sample]
+        t0 = time.time()
+        g.search(sub, L_op, K, entry, threads=threads)
+        times.append(time.time() - t0)
+    qps = sample * len(times) / sum(times)
+    line = {
+        "metric": "QPS at recall@10>=0.95 (1Mx128), reduced-prec+rerank vs FP32 plain; p99 latency",
+        "value": round(qps, 1), "unit": "queries/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * statistics.mean(times), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded clipped Gaussian mixture)", "impl": "reference",
+        "config": {"workload": f"{n}x{DIM} integer-valued f32, 1000-cluster mixture; {nq} queries; "
+                               f"build R={R} L={L_BUILD} alpha={ALPHA} batches of {BATCH}; k={K}",
+                   "L": L_op, "graph": "built on the GPU (untimed), searched on the CPU"},
+        "cpu_baseline": {"value": round(qps, 1), "unit": "queries/s", "cores": threads, "kind": "port",
+                         "sample": f"{sample} queries per step, oracle/vann_oracle.c GreedySearch"},
+        "e2e": {"value": round(qps, 1), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    if "--impl" in sys.argv and sys.argv[sys.argv.index("--impl") + 1] == "reference":
+        sys.exit(main_reference())
+    sys.exit(main())

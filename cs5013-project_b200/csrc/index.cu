@@ -1,0 +1,768 @@
+// index.cu -- host-side index object behind the C ABI (include/vann.h).
+//
+// Replaces the reference's Vamana<T> class and its GraphT / InsertList /
+// DeleteList members (vamana/include/vamana.cuh:36-146, vamana_impl.cuh,
+// insert_list.cuh, delete_list.cuh).  Differences by design: many indexes per
+// process (no __managed__ globals), capacity allocated once (no realloc + copy
+// per patch), every call stream-ordered and returning a status instead of
+// exit(), structure-of-arrays storage with 64-bit offsets, and inserts that
+// reach the graph in the same call.
+#include <cub/cub.cuh>
+
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/vann.h"
+#include "common.cuh"
+#include "kernels.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Fail {
+    vann_status st;
+};
+
+void set_err(const std::string& m) { g_last_error = m; }
+
+#define VCHECK(call)                                                                  \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess) {                                                      \
+            set_err(std::string(#call) + ": " + cudaGetErrorString(e_));              \
+            throw Fail{e_ == cudaErrorMemoryAllocation ? VANN_ERR_OOM : VANN_ERR_CUDA}; \
+        }                                                                             \
+    } while (0)
+
+#define VREQUIRE(cond, code, msg) \
+    do {                          \
+        if (!(cond)) {            \
+            set_err(msg);         \
+            throw Fail{code};     \
+        }                         \
+    } while (0)
+
+// grow-only device buffer
+struct DevBuf {
+    void*  p     = nullptr;
+    size_t bytes = 0;
+    void   ensure(size_t b) {
+        if (b <= bytes) return;
+        if (p) cudaFree(p);
+        p     = nullptr;
+        bytes = 0;
+        VCHECK(cudaMalloc(&p, b));
+        bytes = b;
+    }
+    template <typename T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p     = nullptr;
+        bytes = 0;
+    }
+};
+
+__global__ void scatter_rows_kernel(const float* src, const uint32_t* ids, uint64_t n, uint32_t D,
+                                    float* dst, uint32_t* deg, uint32_t* tomb) {
+    uint64_t r    = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
+    uint32_t lane = threadIdx.x & 31u;
+    if (r >= n) return;
+    uint32_t id = ids[r];
+    for (uint32_t i = lane; i < D; i += 32) dst[(uint64_t)id * D + i] = src[r * D + i];
+    if (lane == 0) {
+        deg[id] = 0;
+        atomicAnd(tomb + (id >> 5), ~(1u << (id & 31u)));
+    }
+}
+
+__global__ void gather_rows_kernel(const float* src, const uint32_t* ids, uint64_t n, uint32_t D,
+                                   float* dst) {
+    uint64_t r    = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
+    uint32_t lane = threadIdx.x & 31u;
+    if (r >= n) return;
+    uint32_t id = ids[r];
+    for (uint32_t i = lane; i < D; i += 32) dst[r * D + i] = src[(uint64_t)id * D + i];
+}
+
+__global__ void clear_deg_kernel(const uint32_t* ids, uint64_t n, uint32_t* deg) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < n) deg[ids[i]] = 0;
+}
+
+constexpr int kCounterRing = 256;
+
+}  // namespace
+
+struct vann_index {
+    vann_params p{};
+    int         device  = 0;
+    int         num_sms = 148;
+    uint64_t    size    = 0;
+    uint64_t    n_deleted = 0;  // tombstoned and not yet freed
+    uint32_t    entry   = vann::kNone;
+    bool        consistent = false;
+
+    float*    vecs  = nullptr;
+    void*     store[4] = {nullptr, nullptr, nullptr, nullptr};
+    float*    fp8_scale = nullptr;
+    uint32_t* deg  = nullptr;
+    uint32_t* adj  = nullptr;
+    uint32_t* tomb = nullptr;
+    uint32_t* counters = nullptr;  // ring of work counters
+    uint32_t* status   = nullptr;
+    int       ring_pos = 0;
+    size_t    held     = 0;
+
+    std::vector<uint32_t> free_ids;  // consolidated ids, reused by inserts
+
+    DevBuf vis_ids, vis_d, vis_n, nodes, e_keys, e_vals, e_keys2, e_vals2, counts, offsets, cub_tmp,
+        medoid_ws, gather, cand, cand_n, cand_d, list_n, out_tmp;
+
+    void alloc(void** ptr, size_t bytes) {
+        VCHECK(cudaMalloc(ptr, bytes));
+        held += bytes;
+    }
+    ~vann_index() {
+        cudaFree(vecs);
+        for (void* s : store) cudaFree(s);
+        cudaFree(fp8_scale);
+        cudaFree(deg);
+        cudaFree(adj);
+        cudaFree(tomb);
+        cudaFree(counters);
+        cudaFree(status);
+        for (DevBuf* b : {&vis_ids, &vis_d, &vis_n, &nodes, &e_keys, &e_vals, &e_keys2, &e_vals2,
+                          &counts, &offsets, &cub_tmp, &medoid_ws, &gather, &cand, &cand_n, &cand_d,
+                          &list_n, &out_tmp})
+            b->release();
+    }
+
+    uint32_t* next_counter(cudaStream_t st) {
+        uint32_t* c = counters + (ring_pos++ % kCounterRing) * 32;
+        VCHECK(cudaMemsetAsync(c, 0, sizeof(uint32_t), st));
+        return c;
+    }
+
+    uint64_t tomb_words() const { return (p.capacity + 31) / 32; }
+
+    void convert_rows(uint64_t first, uint64_t rows, cudaStream_t st) {
+        for (int s = 1; s < 4; ++s) {
+            if (!store[s]) continue;
+            size_t esz = s == 1 ? 2 : 1;
+            void*  dst = static_cast<char*>(store[s]) + first * p.dim * esz;
+            VCHECK(vann::launch_convert(vecs + first * p.dim, dst, s == 2 ? fp8_scale + first : nullptr,
+                                        rows, p.dim, s, st));
+        }
+    }
+
+    uint32_t medoid(uint64_t n, cudaStream_t st) {
+        const size_t mean_bytes = (sizeof(double) * p.dim + 15) & ~size_t(15);
+        medoid_ws.ensure(mean_bytes + 16);
+        double*             mean = medoid_ws.as<double>();
+        unsigned long long* best =
+            reinterpret_cast<unsigned long long*>(static_cast<char*>(medoid_ws.p) + mean_bytes);
+        VCHECK(vann::launch_medoid(vecs, n, p.dim, mean, best, st));
+        unsigned long long hb[2];
+        VCHECK(cudaMemcpyAsync(hb, best, sizeof(hb), cudaMemcpyDeviceToHost, st));
+        VCHECK(cudaStreamSynchronize(st));
+        return (uint32_t)hb[1];
+    }
+
+    // One Vamana batch over the nodes in d_nodes (vectors already stored):
+    // GreedySearch from the entry, out-prune, reverse edges, re-prune.
+    void vamana_batch(const uint32_t* d_nodes, uint64_t count, const float* d_q, uint32_t skip_mode,
+                      uint32_t skip_base, bool all_nodes, cudaStream_t st) {
+        if (count == 0) return;
+        const uint32_t R  = p.degree;
+        const uint32_t MV = p.max_visited;
+        vis_ids.ensure(sizeof(uint32_t) * count * MV);
+        vis_d.ensure(sizeof(float) * count * MV);
+        vis_n.ensure(sizeof(uint32_t) * count);
+
+        vann::SearchArgs a{};
+        a.store = vecs;
+        a.vecs_f32 = vecs;
+        a.deg = deg;
+        a.adj = adj;
+        a.R = R;
+        a.tomb = tomb;
+        a.queries = d_q;
+        a.nq = count;
+        a.D = p.dim;
+        a.L = p.build_L;
+        a.k = 0;
+        a.entry = entry;
+        a.max_hops = 1000000u;
+        a.skip_mode = skip_mode;
+        a.skip_base = skip_base;
+        a.vis_ids = vis_ids.as<uint32_t>();
+        a.vis_d = vis_d.as<float>();
+        a.vis_n = vis_n.as<uint32_t>();
+        a.max_visited = MV;
+        a.counter = next_counter(st);
+        a.status = status;
+        VCHECK(vann::launch_search(a, 0, num_sms, st));
+
+        vann::PruneArgs pa{};
+        pa.vecs = vecs;
+        pa.D = p.dim;
+        pa.deg = deg;
+        pa.adj = adj;
+        pa.R = R;
+        pa.alpha = p.alpha;
+        pa.cap = MV;
+        pa.node_ids = d_nodes;
+        pa.n_nodes = count;
+        pa.a_ids = vis_ids.as<uint32_t>();
+        pa.a_d = vis_d.as<float>();
+        pa.a_n = vis_n.as<uint32_t>();
+        pa.a_stride = MV;
+        pa.use_b = 1;
+        pa.consistent = 0;
+        pa.counter = next_counter(st);
+        pa.status = status;
+        VCHECK(vann::launch_prune(pa, num_sms, st));
+
+        // reverse edges, sorted by target with sources in batch order (stable)
+        const uint64_t ne = count * R;
+        e_keys.ensure(sizeof(uint32_t) * ne);
+        e_vals.ensure(sizeof(uint32_t) * ne);
+        e_keys2.ensure(sizeof(uint32_t) * ne);
+        e_vals2.ensure(sizeof(uint32_t) * ne);
+        // sized by capacity once, so no buffer is freed while earlier batches run
+        counts.ensure(sizeof(uint32_t) * (p.capacity + 1));
+        offsets.ensure(sizeof(uint32_t) * (p.capacity + 1));
+        VCHECK(cudaMemsetAsync(counts.p, 0, sizeof(uint32_t) * (size + 1), st));
+        VCHECK(vann::launch_edges(d_nodes, count, deg, adj, R, e_keys.as<uint32_t>(),
+                                  e_vals.as<uint32_t>(), counts.as<uint32_t>(), st));
+        const int end_bit = 32;  // padded slots carry UINT32_MAX keys
+        size_t tmp_sort = 0, tmp_scan = 0;
+        VCHECK(cub::DeviceRadixSort::SortPairs(nullptr, tmp_sort, e_keys.as<uint32_t>(),
+                                               e_keys2.as<uint32_t>(), e_vals.as<uint32_t>(),
+                                               e_vals2.as<uint32_t>(), (int)ne, 0, end_bit, st));
+        VCHECK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_scan, counts.as<uint32_t>(),
+                                             offsets.as<uint32_t>(), (int)(size + 1), st));
+        cub_tmp.ensure(std::max(tmp_sort, tmp_scan));
+        size_t t1 = cub_tmp.bytes;
+        VCHECK(cub::DeviceRadixSort::SortPairs(cub_tmp.p, t1, e_keys.as<uint32_t>(),
+                                               e_keys2.as<uint32_t>(), e_vals.as<uint32_t>(),
+                                               e_vals2.as<uint32_t>(), (int)ne, 0, end_bit, st));
+        size_t t2 = cub_tmp.bytes;
+        VCHECK(cub::DeviceScan::ExclusiveSum(cub_tmp.p, t2, counts.as<uint32_t>(),
+                                             offsets.as<uint32_t>(), (int)(size + 1), st));
+
+        const bool consistent_rev = consistent || all_nodes;
+        vann::PruneArgs ra{};
+        ra.vecs = vecs;
+        ra.D = p.dim;
+        ra.deg = deg;
+        ra.adj = adj;
+        ra.R = R;
+        ra.alpha = p.alpha;
+        ra.cap = p.max_reverse;
+        ra.node_ids = nullptr;
+        ra.n_nodes = size;
+        ra.csr_off = offsets.as<uint32_t>();
+        ra.csr_cnt = counts.as<uint32_t>();
+        ra.csr_src = e_vals2.as<uint32_t>();
+        ra.use_b = 1;
+        ra.skip_empty = consistent_rev ? 1 : 0;
+        ra.consistent = consistent_rev ? 1 : 0;
+        ra.counter = next_counter(st);
+        ra.status = status;
+        VCHECK(vann::launch_prune(ra, num_sms, st));
+        consistent = true;
+    }
+};
+
+namespace {
+
+vann_status guard(const std::function<void()>& f) {
+    try {
+        f();
+        return VANN_OK;
+    } catch (const Fail& e) {
+        return e.st;
+    } catch (const std::bad_alloc&) {
+        set_err("host allocation failed");
+        return VANN_ERR_OOM;
+    } catch (...) {
+        set_err("unexpected exception");
+        return VANN_ERR_INVALID;
+    }
+}
+
+cudaStream_t S(void* s) { return static_cast<cudaStream_t>(s); }
+
+}  // namespace
+
+extern "C" {
+
+const char* vann_status_string(vann_status s) {
+    switch (s) {
+        case VANN_OK: return "ok";
+        case VANN_ERR_INVALID: return "invalid argument";
+        case VANN_ERR_CUDA: return "CUDA error";
+        case VANN_ERR_CAPACITY: return "capacity exhausted";
+        case VANN_ERR_IO: return "I/O error";
+        case VANN_ERR_HOP_LIMIT: return "hop limit reached";
+        case VANN_ERR_NOT_FOUND: return "not found";
+        case VANN_ERR_TIMEOUT: return "timeout";
+        case VANN_ERR_OOM: return "out of memory";
+        case VANN_ERR_UNSUPPORTED: return "unsupported";
+        case VANN_ERR_STATE: return "invalid state";
+    }
+    return "unknown";
+}
+
+const char* vann_last_error(void) { return g_last_error.c_str(); }
+int         vann_abi_version(void) { return VANN_ABI_VERSION; }
+
+vann_status vann_create(const vann_params* params, vann_index** out) {
+    return guard([&] {
+        VREQUIRE(params && out, VANN_ERR_INVALID, "null argument");
+        const vann_params& p = *params;
+        VREQUIRE(p.dim >= 4 && p.dim % 4 == 0 && p.dim <= 512, VANN_ERR_UNSUPPORTED,
+                 "dim must be a multiple of 4 in [4, 512]");
+        VREQUIRE(p.degree >= 1 && p.degree <= 128, VANN_ERR_UNSUPPORTED, "degree must be in [1, 128]");
+        VREQUIRE(p.build_L >= 1 && p.build_L <= 1024, VANN_ERR_INVALID, "build_L must be in [1, 1024]");
+        VREQUIRE(p.capacity >= 1 && p.capacity < 0x7fffffffull, VANN_ERR_INVALID,
+                 "capacity must be in [1, 2^31-1)");
+        VREQUIRE(p.max_visited >= 1 && p.max_visited <= 2048, VANN_ERR_INVALID,
+                 "max_visited must be in [1, 2048]");
+        VREQUIRE(p.max_reverse >= 1 && p.max_reverse <= 2048, VANN_ERR_INVALID,
+                 "max_reverse must be in [1, 2048]");
+        VREQUIRE(p.alpha >= 1.0f, VANN_ERR_INVALID, "alpha must be >= 1");
+        auto* h = new vann_index();
+        try {
+            h->p = p;
+            VCHECK(cudaGetDevice(&h->device));
+            VCHECK(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
+            const uint64_t C = p.capacity;
+            h->alloc((void**)&h->vecs, sizeof(float) * C * p.dim);
+            if (p.stores & (1u << VANN_STORE_BF16)) h->alloc(&h->store[1], 2ull * C * p.dim);
+            if (p.stores & (1u << VANN_STORE_FP8)) {
+                h->alloc(&h->store[2], 1ull * C * p.dim);
+                h->alloc((void**)&h->fp8_scale, sizeof(float) * C);
+            }
+            if (p.stores & (1u << VANN_STORE_U8)) h->alloc(&h->store[3], 1ull * C * p.dim);
+            h->store[0] = h->vecs;
+            h->alloc((void**)&h->deg, sizeof(uint32_t) * C);
+            h->alloc((void**)&h->adj, sizeof(uint32_t) * C * p.degree);
+            h->alloc((void**)&h->tomb, sizeof(uint32_t) * h->tomb_words());
+            h->alloc((void**)&h->counters, sizeof(uint32_t) * 32 * kCounterRing);
+            h->alloc((void**)&h->status, sizeof(uint32_t) * 32);
+            VCHECK(cudaMemset(h->deg, 0, sizeof(uint32_t) * C));
+            VCHECK(cudaMemset(h->tomb, 0, sizeof(uint32_t) * h->tomb_words()));
+            VCHECK(cudaMemset(h->status, 0, sizeof(uint32_t) * 32));
+            VCHECK(cudaDeviceSynchronize());
+        } catch (...) {
+            h->store[0] = nullptr;
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+vann_status vann_destroy(vann_index* h) {
+    return guard([&] {
+        if (!h) return;
+        cudaDeviceSynchronize();
+        h->store[0] = nullptr;  // alias of vecs
+        delete h;
+    });
+}
+
+vann_status vann_get_info(const vann_index* h, vann_info* out) {
+    return guard([&] {
+        VREQUIRE(h && out, VANN_ERR_INVALID, "null argument");
+        out->size = h->size;
+        out->capacity = h->p.capacity;
+        out->live = h->size - h->n_deleted - h->free_ids.size();
+        out->free_ids = h->free_ids.size();
+        out->entry = h->entry;
+        out->dim = h->p.dim;
+        out->degree = h->p.degree;
+        out->consistent = h->consistent ? 1u : 0u;
+        out->device_bytes = h->held;
+    });
+}
+
+vann_status vann_set_graph(vann_index* h, const float* h_vecs, const uint32_t* h_deg,
+                           const uint32_t* h_adj, uint64_t n, uint32_t entry, uint32_t consistent) {
+    return guard([&] {
+        VREQUIRE(h && h_vecs && h_deg && h_adj, VANN_ERR_INVALID, "null argument");
+        VREQUIRE(n <= h->p.capacity, VANN_ERR_CAPACITY, "n exceeds capacity");
+        VREQUIRE(n == 0 || entry < n, VANN_ERR_INVALID, "entry must be < n");
+        const uint32_t R = h->p.degree;
+        for (uint64_t i = 0; i < n; ++i) {
+            VREQUIRE(h_deg[i] <= R, VANN_ERR_INVALID, "degree exceeds R");
+            for (uint32_t j = 0; j < h_deg[i]; ++j)
+                VREQUIRE(h_adj[i * R + j] < n, VANN_ERR_INVALID, "neighbour id out of range");
+        }
+        VCHECK(cudaMemcpy(h->vecs, h_vecs, sizeof(float) * n * h->p.dim, cudaMemcpyHostToDevice));
+        VCHECK(cudaMemcpy(h->deg, h_deg, sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+        VCHECK(cudaMemcpy(h->adj, h_adj, sizeof(uint32_t) * n * R, cudaMemcpyHostToDevice));
+        VCHECK(cudaMemset(h->tomb, 0, sizeof(uint32_t) * h->tomb_words()));
+        h->convert_rows(0, n, 0);
+        VCHECK(cudaDeviceSynchronize());
+        h->size = n;
+        h->n_deleted = 0;
+        h->free_ids.clear();
+        h->entry = entry;
+        h->consistent = consistent != 0;
+    });
+}
+
+vann_status vann_get_graph(vann_index* h, float* h_vecs, uint32_t* h_deg, uint32_t* h_adj) {
+    return guard([&] {
+        VREQUIRE(h, VANN_ERR_INVALID, "null argument");
+        VCHECK(cudaDeviceSynchronize());
+        if (h_vecs)
+            VCHECK(cudaMemcpy(h_vecs, h->vecs, sizeof(float) * h->size * h->p.dim, cudaMemcpyDeviceToHost));
+        if (h_deg) VCHECK(cudaMemcpy(h_deg, h->deg, sizeof(uint32_t) * h->size, cudaMemcpyDeviceToHost));
+        if (h_adj)
+            VCHECK(cudaMemcpy(h_adj, h->adj, sizeof(uint32_t) * h->size * h->p.degree,
+                              cudaMemcpyDeviceToHost));
+    });
+}
+
+vann_status vann_load_graph(vann_index* h, const char* path, uint64_t n, uint32_t entry) {
+    return guard([&] {
+        VREQUIRE(h && path, VANN_ERR_INVALID, "null argument");
+        const uint32_t D = h->p.dim, R = h->p.degree;
+        const size_t   rec = 4ull * D + 4 + 4ull * R;
+        FILE*          f   = fopen(path, "rb");
+        VREQUIRE(f, VANN_ERR_IO, std::string("cannot open ") + path);
+        std::vector<unsigned char> buf(rec * n);
+        size_t got = fread(buf.data(), rec, n, f);
+        fclose(f);
+        VREQUIRE(got == n, VANN_ERR_IO, "short read");
+        std::vector<float>    v(n * D);
+        std::vector<uint32_t> d(n), a(n * R);
+        for (uint64_t i = 0; i < n; ++i) {
+            const unsigned char* r = buf.data() + i * rec;
+            memcpy(&v[i * D], r, 4ull * D);
+            memcpy(&d[i], r + 4ull * D, 4);
+            memcpy(&a[i * R], r + 4ull * D + 4, 4ull * R);
+            // unused slots of the file may hold anything; keep them in range
+            for (uint32_t j = d[i] < R ? d[i] : R; j < R; ++j) a[i * R + j] = 0;
+        }
+        vann_status s = vann_set_graph(h, v.data(), d.data(), a.data(), n, entry, 0);
+        VREQUIRE(s == VANN_OK, s, g_last_error);
+    });
+}
+
+vann_status vann_save_graph(vann_index* h, const char* path) {
+    return guard([&] {
+        VREQUIRE(h && path, VANN_ERR_INVALID, "null argument");
+        const uint32_t D = h->p.dim, R = h->p.degree;
+        const uint64_t n = h->size;
+        std::vector<float>    v(n * D);
+        std::vector<uint32_t> d(n), a(n * R);
+        vann_status           s = vann_get_graph(h, v.data(), d.data(), a.data());
+        VREQUIRE(s == VANN_OK, s, g_last_error);
+        const size_t               rec = 4ull * D + 4 + 4ull * R;
+        std::vector<unsigned char> buf(rec * n);
+        for (uint64_t i = 0; i < n; ++i) {
+            unsigned char* r = buf.data() + i * rec;
+            memcpy(r, &v[i * D], 4ull * D);
+            memcpy(r + 4ull * D, &d[i], 4);
+            memset(r + 4ull * D + 4, 0, 4ull * R);
+            memcpy(r + 4ull * D + 4, &a[i * R], 4ull * d[i]);
+        }
+        FILE* f = fopen(path, "wb");
+        VREQUIRE(f, VANN_ERR_IO, std::string("cannot open ") + path);
+        size_t put = fwrite(buf.data(), rec, n, f);
+        fclose(f);
+        VREQUIRE(put == n, VANN_ERR_IO, "short write");
+    });
+}
+
+vann_status vann_build(vann_index* h, const float* d_vecs, uint64_t n, uint64_t batch, uint64_t seed,
+                       uint32_t entry, void* stream) {
+    return guard([&] {
+        VREQUIRE(h && (d_vecs || n == 0), VANN_ERR_INVALID, "null argument");
+        VREQUIRE(n <= h->p.capacity, VANN_ERR_CAPACITY, "n exceeds capacity");
+        cudaStream_t   st = S(stream);
+        const uint32_t D = h->p.dim, R = h->p.degree;
+        h->size = 0;
+        h->n_deleted = 0;
+        h->free_ids.clear();
+        h->consistent = false;
+        if (n == 0) return;
+        VCHECK(cudaMemcpyAsync(h->vecs, d_vecs, sizeof(float) * n * D, cudaMemcpyDeviceToDevice, st));
+        VCHECK(cudaMemsetAsync(h->tomb, 0, sizeof(uint32_t) * h->tomb_words(), st));
+        VCHECK(cudaMemsetAsync(h->deg, 0, sizeof(uint32_t) * n, st));
+        h->convert_rows(0, n, st);
+        const uint64_t first = (batch == 0 || batch >= n) ? n : batch;
+        VCHECK(vann::launch_random_graph(h->deg, h->adj, 0, first, first, R, seed, st));
+        h->size  = first;
+        h->entry = entry != vann::kNone ? entry : h->medoid(first, st);
+        VREQUIRE(h->entry < first, VANN_ERR_INVALID, "entry must be inside the first batch");
+        const bool parity = (h->p.flags & VANN_QUIRK_SKIP_BATCH_INDEX) != 0;
+        const uint64_t step = first;
+        h->nodes.ensure(sizeof(uint32_t) * (batch == 0 || batch >= n ? n : batch));
+        VCHECK(vann::launch_iota(h->nodes.as<uint32_t>(), first, 0, st));
+        h->vamana_batch(h->nodes.as<uint32_t>(), first, h->vecs, parity ? 1u : 2u, 0u, true, st);
+        for (uint64_t s = first; s < n; s += step) {
+            uint64_t c = std::min(step, n - s);
+            h->size    = s + c;
+            VCHECK(vann::launch_iota(h->nodes.as<uint32_t>(), c, (uint32_t)s, st));
+            h->vamana_batch(h->nodes.as<uint32_t>(), c, h->vecs + s * D, parity ? 1u : 0u, 0u, false, st);
+        }
+        VCHECK(cudaStreamSynchronize(st));
+        VCHECK(cudaGetLastError());
+    });
+}
+
+vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq,
+                              const vann_search_params* sp, uint32_t* d_ids, float* d_dists,
+                              uint32_t* d_hops, uint32_t* d_evals, uint32_t* d_adjw, void* stream) {
+    return guard([&] {
+        VREQUIRE(h && sp && (nq == 0 || (d_queries && d_ids && d_dists)), VANN_ERR_INVALID,
+                 "null argument");
+        VREQUIRE(sp->k >= 1 && sp->L >= sp->k && sp->L <= 1024, VANN_ERR_INVALID,
+                 "need 1 <= k <= L <= 1024");
+        VREQUIRE(sp->store < 4 && h->store[sp->store] != nullptr, VANN_ERR_UNSUPPORTED,
+                 "requested store was not enabled at create");
+        VREQUIRE(h->size > 0 && h->entry < h->size, VANN_ERR_STATE, "index is empty");
+        if (nq == 0) return;
+        vann::SearchArgs a{};
+        a.store = h->store[sp->store];
+        a.scale = h->fp8_scale;
+        a.vecs_f32 = h->vecs;
+        a.deg = h->deg;
+        a.adj = h->adj;
+        a.R = h->p.degree;
+        a.tomb = h->n_deleted || !h->free_ids.empty() ? h->tomb : nullptr;
+        a.queries = d_queries;
+        a.nq = nq;
+        a.D = h->p.dim;
+        a.L = sp->L;
+        a.k = sp->k;
+        a.entry = h->entry;
+        a.max_hops = sp->max_hops ? sp->max_hops : 1000000u;
+        a.skip_mode = (sp->flags & VANN_QUIRK_SKIP_BATCH_INDEX) ? 1u : 0u;
+        a.rerank = sp->rerank ? 1 : 0;
+        a.out_ids = d_ids;
+        a.out_d = d_dists;
+        a.hops_out = d_hops;
+        a.evals_out = d_evals;
+        a.adjw_out = d_adjw;
+        a.counter = h->next_counter(S(stream));
+        a.status = h->status;
+        VCHECK(vann::launch_search(a, (int)sp->store, h->num_sms, S(stream)));
+    });
+}
+
+vann_status vann_search(vann_index* h, const float* d_queries, uint64_t nq,
+                        const vann_search_params* sp, uint32_t* d_ids, float* d_dists, void* stream) {
+    return vann_search_stats(h, d_queries, nq, sp, d_ids, d_dists, nullptr, nullptr, nullptr, stream);
+}
+
+vann_status vann_sync(vann_index* h, void* stream) {
+    vann_status result = VANN_OK;
+    vann_status s = guard([&] {
+        VREQUIRE(h, VANN_ERR_INVALID, "null argument");
+        VCHECK(cudaStreamSynchronize(S(stream)));
+        uint32_t w = 0;
+        VCHECK(cudaMemcpy(&w, h->status, sizeof(w), cudaMemcpyDeviceToHost));
+        VCHECK(cudaMemset(h->status, 0, sizeof(uint32_t)));
+        if (w & vann::kStatusHopLimit) {
+            set_err("a search stopped at its hop limit");
+            result = VANN_ERR_HOP_LIMIT;
+        }
+    });
+    return s != VANN_OK ? s : result;
+}
+
+vann_status vann_insert(vann_index* h, const float* d_vecs, uint64_t n, uint32_t* d_ids_out,
+                        void* stream) {
+    return guard([&] {
+        VREQUIRE(h && (d_vecs || n == 0), VANN_ERR_INVALID, "null argument");
+        VREQUIRE(h->size > 0, VANN_ERR_STATE, "build or load a graph first");
+        if (n == 0) return;
+        const uint64_t reuse = std::min<uint64_t>(n, h->free_ids.size());
+        VREQUIRE(h->size + (n - reuse) <= h->p.capacity, VANN_ERR_CAPACITY, "capacity exhausted");
+        cudaStream_t   st = S(stream);
+        const uint32_t D  = h->p.dim;
+        std::vector<uint32_t> ids(n);
+        for (uint64_t i = 0; i < reuse; ++i) {
+            ids[i] = h->free_ids.back();
+            h->free_ids.pop_back();
+        }
+        for (uint64_t i = reuse; i < n; ++i) ids[i] = (uint32_t)(h->size + (i - reuse));
+        h->nodes.ensure(sizeof(uint32_t) * n);
+        VCHECK(cudaMemcpyAsync(h->nodes.p, ids.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st));
+        scatter_rows_kernel<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(d_vecs, h->nodes.as<uint32_t>(), n,
+                                                                     D, h->vecs, h->deg, h->tomb);
+        VCHECK(cudaGetLastError());
+        if (reuse == 0) {
+            h->convert_rows(h->size, n, st);
+        } else {
+            // reused ids are scattered: convert every touched row one by one
+            for (uint64_t i = 0; i < n; ++i) h->convert_rows(ids[i], 1, st);
+        }
+        h->size += n - reuse;
+        const bool parity = (h->p.flags & VANN_QUIRK_SKIP_BATCH_INDEX) != 0;
+        h->vamana_batch(h->nodes.as<uint32_t>(), n, d_vecs, parity ? 1u : 0u, 0u, false, st);
+        if (d_ids_out)
+            VCHECK(cudaMemcpyAsync(d_ids_out, h->nodes.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
+        VCHECK(cudaStreamSynchronize(st));
+    });
+}
+
+vann_status vann_delete(vann_index* h, const uint32_t* d_ids, uint64_t n, void* stream) {
+    return guard([&] {
+        VREQUIRE(h && (d_ids || n == 0), VANN_ERR_INVALID, "null argument");
+        VCHECK(vann::launch_set_bits(h->tomb, d_ids, n, h->size, S(stream)));
+        h->n_deleted += n;  // upper bound; recounted at consolidate
+    });
+}
+
+vann_status vann_delete_by_vector(vann_index* h, const float* d_vecs, uint64_t n, int32_t* d_ids_out,
+                                  void* stream) {
+    return guard([&] {
+        VREQUIRE(h && (d_vecs || n == 0), VANN_ERR_INVALID, "null argument");
+        if (n == 0) return;
+        cudaStream_t st = S(stream);
+        h->out_tmp.ensure(sizeof(int32_t) * n);
+        int32_t* res = d_ids_out ? d_ids_out : h->out_tmp.as<int32_t>();
+        VCHECK(vann::launch_find_vectors(h->vecs, h->size, h->p.dim, d_vecs, n, h->tomb, res, st));
+        std::vector<int32_t> hr(n);
+        VCHECK(cudaMemcpyAsync(hr.data(), res, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+        VCHECK(cudaStreamSynchronize(st));
+        std::vector<uint32_t> found;
+        for (int32_t v : hr)
+            if (v >= 0) found.push_back((uint32_t)v);
+        if (!found.empty()) {
+            h->nodes.ensure(sizeof(uint32_t) * found.size());
+            VCHECK(cudaMemcpyAsync(h->nodes.p, found.data(), sizeof(uint32_t) * found.size(),
+                                   cudaMemcpyHostToDevice, st));
+            VCHECK(vann::launch_set_bits(h->tomb, h->nodes.as<uint32_t>(), found.size(), h->size, st));
+            h->n_deleted += found.size();
+            VCHECK(cudaStreamSynchronize(st));
+        }
+        VREQUIRE(found.size() == n, VANN_ERR_NOT_FOUND, "some vectors were not found");
+    });
+}
+
+vann_status vann_consolidate(vann_index* h, void* stream) {
+    return guard([&] {
+        VREQUIRE(h, VANN_ERR_INVALID, "null argument");
+        cudaStream_t   st = S(stream);
+        const uint32_t R  = h->p.degree;
+        // which ids are deleted and not yet free
+        std::vector<uint32_t> tomb(h->tomb_words());
+        VCHECK(cudaMemcpyAsync(tomb.data(), h->tomb, sizeof(uint32_t) * tomb.size(),
+                               cudaMemcpyDeviceToHost, st));
+        VCHECK(cudaStreamSynchronize(st));
+        std::vector<char> is_free(h->size, 0);
+        for (uint32_t f : h->free_ids) is_free[f] = 1;
+        std::vector<uint32_t> dead;
+        for (uint64_t i = 0; i < h->size; ++i)
+            if (((tomb[i >> 5] >> (i & 31)) & 1u) && !is_free[i]) dead.push_back((uint32_t)i);
+        if (dead.empty()) {
+            h->n_deleted = 0;
+            return;
+        }
+        const uint32_t cap = std::min<uint32_t>(2048u, std::max<uint32_t>(h->p.max_visited, 2 * R));
+        h->nodes.ensure(sizeof(uint32_t) * h->size);
+        h->list_n.ensure(sizeof(uint32_t) * 4);
+        h->cand.ensure(sizeof(uint32_t) * h->size * cap);
+        h->cand_d.ensure(sizeof(float) * h->size * cap);
+        h->cand_n.ensure(sizeof(uint32_t) * h->size);
+        VCHECK(cudaMemsetAsync(h->list_n.p, 0, sizeof(uint32_t), st));
+        VCHECK(vann::launch_consolidate_candidates(h->deg, h->adj, R, h->tomb, h->size,
+                                                   h->nodes.as<uint32_t>(), h->list_n.as<uint32_t>(),
+                                                   h->cand.as<uint32_t>(), h->cand_n.as<uint32_t>(),
+                                                   h->cand_d.as<float>(), h->vecs, h->p.dim, cap, st));
+        uint32_t nlist = 0;
+        VCHECK(cudaMemcpyAsync(&nlist, h->list_n.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        VCHECK(cudaStreamSynchronize(st));
+        vann::PruneArgs pa{};
+        pa.vecs = h->vecs;
+        pa.D = h->p.dim;
+        pa.deg = h->deg;
+        pa.adj = h->adj;
+        pa.R = R;
+        pa.alpha = h->p.alpha;
+        pa.cap = cap;
+        pa.node_ids = h->nodes.as<uint32_t>();
+        pa.n_nodes = nlist;
+        pa.a_ids = h->cand.as<uint32_t>();
+        pa.a_d = h->cand_d.as<float>();
+        pa.a_n = h->cand_n.as<uint32_t>();
+        pa.a_stride = cap;
+        pa.use_b = 0;
+        pa.consistent = 0;
+        pa.counter = h->next_counter(st);
+        pa.status = h->status;
+        VCHECK(vann::launch_prune(pa, h->num_sms, st));
+        // free the deleted ids (tombstone stays set until an insert reuses the id)
+        h->nodes.ensure(sizeof(uint32_t) * std::max<size_t>(dead.size(), h->size));
+        VCHECK(cudaMemcpyAsync(h->nodes.p, dead.data(), sizeof(uint32_t) * dead.size(),
+                               cudaMemcpyHostToDevice, st));
+        clear_deg_kernel<<<(unsigned)((dead.size() + 255) / 256), 256, 0, st>>>(
+            h->nodes.as<uint32_t>(), dead.size(), h->deg);
+        VCHECK(cudaGetLastError());
+        // a deleted entry point moves to the live node nearest to its vector,
+        // found by a search that starts from the first live id
+        if ((tomb[h->entry >> 5] >> (h->entry & 31)) & 1u) {
+            uint32_t start = vann::kNone;
+            for (uint64_t i = 0; i < h->size && start == vann::kNone; ++i)
+                if (!((tomb[i >> 5] >> (i & 31)) & 1u)) start = (uint32_t)i;
+            VREQUIRE(start != vann::kNone, VANN_ERR_STATE, "no live node left");
+            h->out_tmp.ensure(sizeof(uint32_t) * 64 + sizeof(float) * h->p.dim);
+            uint32_t* oi = h->out_tmp.as<uint32_t>();
+            float*    od = reinterpret_cast<float*>(oi + 32);
+            float*    qv = reinterpret_cast<float*>(oi + 64);
+            VCHECK(cudaMemcpyAsync(qv, h->vecs + (uint64_t)h->entry * h->p.dim,
+                                   sizeof(float) * h->p.dim, cudaMemcpyDeviceToDevice, st));
+            vann::SearchArgs a{};
+            a.store = h->vecs;
+            a.vecs_f32 = h->vecs;
+            a.deg = h->deg;
+            a.adj = h->adj;
+            a.R = R;
+            a.tomb = h->tomb;
+            a.queries = qv;
+            a.nq = 1;
+            a.D = h->p.dim;
+            a.L = 32;
+            a.k = 32;
+            a.entry = start;
+            a.max_hops = 1000000u;
+            a.out_ids = oi;
+            a.out_d = od;
+            a.counter = h->next_counter(st);
+            a.status = h->status;
+            VCHECK(vann::launch_search(a, 0, h->num_sms, st));
+            std::vector<uint32_t> res(32);
+            VCHECK(cudaMemcpyAsync(res.data(), oi, sizeof(uint32_t) * 32, cudaMemcpyDeviceToHost, st));
+            VCHECK(cudaStreamSynchronize(st));
+            uint32_t ne = start;
+            for (uint32_t r : res)
+                if (r != vann::kNone && !((tomb[r >> 5] >> (r & 31)) & 1u)) {
+                    ne = r;
+                    break;
+                }
+            h->entry = ne;
+        }
+        for (uint32_t d : dead) h->free_ids.push_back(d);
+        h->n_deleted = 0;
+        VCHECK(cudaStreamSynchronize(st));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,95 @@
+// kernels.h -- launch interfaces of the CUDA kernels (host <-> device boundary
+// inside libvann.so; the public C ABI is include/vann.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace vann {
+
+struct SearchArgs {
+    const void*     store;     // traversal copy (F32 / BF16 / FP8 / U8 rows)
+    const float*    scale;     // per-row scale of the FP8 copy
+    const float*    vecs_f32;  // exact rows (rerank)
+    const uint32_t* deg;
+    const uint32_t* adj;
+    uint32_t        R;
+    const uint32_t* tomb;      // tombstone bitmap or null
+    const float*    queries;   // nq x D FP32
+    uint64_t        nq;
+    uint32_t        D;
+    uint32_t        L, k, entry, max_hops;
+    uint32_t        skip_mode;  // 0 none, 1 batch index, 2 skip_base + batch index
+    uint32_t        skip_base;
+    int             rerank;
+    uint32_t*       out_ids;    // nq x k or null
+    float*          out_d;
+    uint32_t*       vis_ids;    // nq x max_visited expansion lists or null
+    float*          vis_d;
+    uint32_t*       vis_n;
+    uint32_t        max_visited;
+    uint32_t*       hops_out;   // per-query hop / distance-evaluation counts or null
+    uint32_t*       evals_out;
+    uint32_t*       adjw_out;   // per-query adjacency words read (sum of parent degrees)
+    uint32_t*       counter;    // zeroed before launch
+    uint32_t*       status;
+};
+
+cudaError_t launch_search(const SearchArgs& a, int store, int num_sms, cudaStream_t st);
+size_t      search_smem_per_warp(uint32_t L, uint32_t R, bool rerank);
+
+// RobustPrune over candidates A (expansion list or reverse entries) merged with
+// B (the node's current out-neighbours).
+struct PruneArgs {
+    const float*    vecs;      // FP32 rows
+    uint32_t        D;
+    uint32_t*       deg;
+    uint32_t*       adj;
+    uint32_t        R;
+    float           alpha;
+    uint32_t        cap;       // merged-list cap (max_visited or max_reverse)
+    // nodes to prune: node_ids[i] for i < n_nodes, or all ids < n_nodes when null
+    const uint32_t* node_ids;
+    uint64_t        n_nodes;
+    // A as per-node lists (out-prune): a_ids/a_d [n_nodes x a_stride], a_n
+    const uint32_t* a_ids;
+    const float*    a_d;
+    const uint32_t* a_n;
+    uint32_t        a_stride;
+    // A as CSR of reverse sources (re-prune): sources of node v in
+    // csr_src[csr_off[v] .. csr_off[v] + csr_cnt[v]) sorted ascending
+    const uint32_t* csr_off;
+    const uint32_t* csr_cnt;
+    const uint32_t* csr_src;
+    int             use_b;       // include the node's current out-neighbours
+    int             skip_empty;  // re-prune: skip nodes without reverse entries
+    int             consistent;  // B lists are alpha-consistent: skip B-B checks
+    uint32_t*       counter;     // work counter, zeroed before launch
+    uint32_t*       status;
+};
+
+cudaError_t launch_prune(const PruneArgs& a, int num_sms, cudaStream_t st);
+
+// graph utilities (graph_ops.cu)
+cudaError_t launch_random_graph(uint32_t* deg, uint32_t* adj, uint64_t first, uint64_t n,
+                                uint64_t range, uint32_t R, uint64_t seed, cudaStream_t st);
+cudaError_t launch_convert(const float* src, void* dst, float* scale, uint64_t rows, uint32_t D,
+                           int store, cudaStream_t st);
+cudaError_t launch_iota(uint32_t* out, uint64_t n, uint32_t first, cudaStream_t st);
+cudaError_t launch_set_bits(uint32_t* bits, const uint32_t* ids, uint64_t n, uint64_t limit,
+                            cudaStream_t st);
+cudaError_t launch_medoid(const float* vecs, uint64_t n, uint32_t D, double* mean_ws,
+                          unsigned long long* best_ws, cudaStream_t st);
+cudaError_t launch_edges(const uint32_t* nodes, uint64_t n_nodes, const uint32_t* deg,
+                         const uint32_t* adj, uint32_t R, uint32_t* keys, uint32_t* vals,
+                         uint32_t* counts, cudaStream_t st);
+cudaError_t launch_find_vectors(const float* vecs, uint64_t n, uint32_t D, const float* q,
+                                uint64_t nq, const uint32_t* tomb, int32_t* out, cudaStream_t st);
+cudaError_t launch_consolidate_candidates(const uint32_t* deg, const uint32_t* adj, uint32_t R,
+                                          const uint32_t* tomb, uint64_t n, uint32_t* node_list,
+                                          uint32_t* n_list, uint32_t* cand, uint32_t* cand_n,
+                                          float* cand_d, const float* vecs, uint32_t D,
+                                          uint32_t cap, cudaStream_t st);
+
+}  // namespace vann

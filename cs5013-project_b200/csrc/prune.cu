@@ -1,0 +1,228 @@
+// prune.cu -- RobustPrune, one warp per node, candidates staged in shared memory.
+//
+// Restates pruneOutNeighbors / pruneReverseEdges (vamana/include/kernels.cuh:
+// 232-356, 626-743) together with the candidate preparation that the reference
+// spreads over getNeighbors, computeDists, sortByDistance and the two merge
+// kernels (:141-229, :567-624):
+//   A = the node's expansion list (out-prune) or its reverse sources (re-prune),
+//   B = the node's current out-neighbours,
+//   candidates = stable sort of A then B by distance to the node (A first on
+//   equal distance), truncated to `cap`;
+//   repeat: p* = first INIT candidate -> out-neighbour; every INIT candidate p
+//   with dist(p*, p) * alpha <= dist(node, p) becomes PRUNED; until R
+//   neighbours or no INIT candidate is left.
+// Distances are squared FP32.  One key (distance bits, candidate index) per
+// candidate gives the stable order in a single bitonic sort.  When B is known
+// to be alpha-consistent (it is the output of an earlier RobustPrune with the
+// same alpha, kept in selection order), a B candidate can never be pruned by a
+// B p*, so those pairs are not evaluated: the decisions are the same, the
+// distance evaluations drop from |C|^2 to about |A| * |C|.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace vann {
+
+constexpr uint8_t kInit = 0, kPruned = 1, kNeighbor = 2, kFromA = 0x10;
+
+struct PruneLayout {
+    uint32_t p2;     // sort size (power of two >= max candidates)
+    uint32_t bytes;  // per warp
+    static PruneLayout make(uint32_t max_cand, uint32_t R) {
+        PruneLayout l;
+        uint32_t    p = 32;
+        while (p < max_cand) p <<= 1;
+        l.p2    = p;
+        l.bytes = 8u * p + 4u * p + 4u * p + p + 4u * R;
+        l.bytes = (l.bytes + 15u) & ~15u;
+        return l;
+    }
+};
+
+template <int NCH>
+__global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, uint32_t warp_bytes) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t wib  = threadIdx.x >> 5;
+    unsigned char* base = smem + (size_t)wib * warp_bytes;
+    uint64_t*      keys = reinterpret_cast<uint64_t*>(base);
+    uint32_t*      cid  = reinterpret_cast<uint32_t*>(base + 8u * p2);
+    float*         cd   = reinterpret_cast<float*>(base + 12u * p2);
+    uint32_t*      sid  = reinterpret_cast<uint32_t*>(cd);  // sorted ids reuse cd
+    uint8_t*       st   = base + 16u * p2;
+    uint32_t*      chosen = reinterpret_cast<uint32_t*>(base + 17u * p2);
+    const uint32_t R    = a.R;
+    const bool     rev  = a.csr_off != nullptr;
+    const uint32_t chunk = 32u;
+
+    for (;;) {
+        uint32_t w0 = 0;
+        if (lane == 0) w0 = atomicAdd(a.counter, chunk);
+        w0 = __shfl_sync(0xffffffffu, w0, 0);
+        if (w0 >= a.n_nodes) break;
+        uint32_t wend = (uint32_t)min((uint64_t)w0 + chunk, a.n_nodes);
+        // which of the chunk's nodes have work
+        uint32_t wi   = w0 + lane;
+        bool     has  = wi < wend;
+        uint32_t mynode = 0;
+        if (has) {
+            mynode = a.node_ids ? __ldg(a.node_ids + wi) : wi;
+            if (rev && a.skip_empty && __ldg(a.csr_cnt + mynode) == 0u) has = false;
+        }
+        uint32_t todo = __ballot_sync(0xffffffffu, has);
+        while (todo) {
+            const uint32_t src  = __ffs(todo) - 1u;
+            todo &= todo - 1u;
+            const uint32_t w    = w0 + src;
+            const uint32_t node = __shfl_sync(0xffffffffu, mynode, src);
+
+            float4 nv[NCH];
+            load_query_f32<NCH>(nv, a.vecs + (uint64_t)node * a.D, a.D, lane);
+
+            // --- candidates: A then B
+            uint32_t nA = 0, aoff = 0;
+            if (rev) {
+                nA   = __ldg(a.csr_cnt + node);
+                aoff = __ldg(a.csr_off + node);
+                nA   = min(nA, a.cap);
+            } else {
+                nA = min(__ldg(a.a_n + w), a.a_stride);
+            }
+            uint32_t nB = a.use_b ? min(__ldg(a.deg + node), R) : 0u;
+            uint32_t nc = nA + nB;
+            for (uint32_t i = lane; i < nc; i += 32) {
+                uint32_t id;
+                float    d = 0.f;
+                if (i < nA) {
+                    if (rev) {
+                        id = __ldg(a.csr_src + aoff + i);
+                    } else {
+                        id = __ldg(a.a_ids + (uint64_t)w * a.a_stride + i);
+                        d  = __ldg(a.a_d + (uint64_t)w * a.a_stride + i);
+                    }
+                } else {
+                    id = __ldg(a.adj + (uint64_t)node * R + (i - nA));
+                }
+                cid[i] = id;
+                cd[i]  = d;
+            }
+            __syncwarp();
+            // distances to the node for the reverse sources and B
+            const uint32_t dstart = rev ? 0u : nA;
+            uint32_t       ids8[8];
+            for (uint32_t g0 = dstart; g0 < nc; g0 += 8) {
+                int gc = (int)min(8u, nc - g0);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) ids8[j] = j < gc ? cid[g0 + j] : 0u;
+                float    y  = dist8<StoreF32, NCH>(nv, a.vecs, nullptr, ids8, gc, a.D, lane);
+                uint32_t vi = vidx_of_lane(lane);
+                if ((lane & 3u) == 0 && (int)vi < gc) cd[g0 + vi] = y;
+            }
+            __syncwarp();
+            uint32_t ns = 32;
+            while (ns < nc) ns <<= 1;
+            for (uint32_t i = lane; i < ns; i += 32) keys[i] = i < nc ? make_key(cd[i], i) : ~0ull;
+            __syncwarp();
+            warp_bitonic_sort_smem(keys, ns, lane);
+            const uint32_t ncap = min(nc, a.cap);
+            for (uint32_t t = lane; t < ncap; t += 32) {
+                uint32_t idx = (uint32_t)keys[t];
+                sid[t]       = cid[idx];
+                st[t]        = idx < nA ? kFromA : 0;
+            }
+            __syncwarp();
+
+            // --- RobustPrune
+            uint32_t ndeg = 0, first = 0;
+            while (ndeg < R) {
+                int found = -1;
+                for (uint32_t c0 = first; c0 < ncap; c0 += 32) {
+                    uint32_t i  = c0 + lane;
+                    bool     in = i < ncap && (st[i] & 3u) == kInit;
+                    uint32_t m  = __ballot_sync(0xffffffffu, in);
+                    if (m) {
+                        found = (int)(c0 + __ffs(m) - 1);
+                        break;
+                    }
+                }
+                if (found < 0) break;
+                const uint32_t ps    = sid[found];
+                const bool     ps_a  = (st[found] & kFromA) != 0;
+                __syncwarp();
+                if (lane == 0) {
+                    st[found]    = (uint8_t)(kNeighbor | (ps_a ? kFromA : 0));
+                    chosen[ndeg] = ps;
+                }
+                ++ndeg;
+                first = (uint32_t)found + 1u;
+                __syncwarp();
+                if (ndeg >= R) break;
+
+                float4 pv[NCH];
+                load_query_f32<NCH>(pv, a.vecs + (uint64_t)ps * a.D, a.D, lane);
+                for (uint32_t c0 = first; c0 < ncap; c0 += 32) {
+                    uint32_t i    = c0 + lane;
+                    bool     need = false;
+                    if (i < ncap) {
+                        uint8_t s = st[i];
+                        need      = (s & 3u) == kInit && (!a.consistent || ps_a || (s & kFromA));
+                    }
+                    uint32_t m = __ballot_sync(0xffffffffu, need);
+                    while (m) {
+                        uint32_t pos8[8];
+                        int      gc = 0;
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            if (m) {
+                                pos8[j] = c0 + __ffs(m) - 1u;
+                                m &= m - 1u;
+                                ++gc;
+                            } else {
+                                pos8[j] = c0;
+                            }
+                            ids8[j] = sid[pos8[j]];
+                        }
+                        float    y  = dist8<StoreF32, NCH>(pv, a.vecs, nullptr, ids8, gc, a.D, lane);
+                        uint32_t vi = vidx_of_lane(lane);
+                        if ((lane & 3u) == 0 && (int)vi < gc) {
+                            uint32_t t = pos8[vi];
+                            if (y * a.alpha <= key_dist(keys[t])) st[t] = (uint8_t)(kPruned | (st[t] & kFromA));
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+            // rewrite the node's adjacency (in place, like the reference)
+            for (uint32_t t = lane; t < ndeg; t += 32) a.adj[(uint64_t)node * R + t] = chosen[t];
+            if (lane == 0) a.deg[node] = ndeg;
+            __syncwarp();
+        }
+    }
+}
+
+cudaError_t launch_prune(const PruneArgs& a, int num_sms, cudaStream_t st) {
+    if (a.n_nodes == 0) return cudaSuccess;
+    uint32_t    maxa = a.csr_off ? a.cap : a.a_stride;
+    PruneLayout lay  = PruneLayout::make(maxa + a.R, a.R);
+    const int   warps = 4;
+    size_t      smem  = (size_t)lay.bytes * warps;
+    void (*kern)(PruneArgs, uint32_t, uint32_t);
+    if (a.D <= 128)
+        kern = prune_kernel<1>;
+    else if (a.D <= 256)
+        kern = prune_kernel<2>;
+    else
+        kern = prune_kernel<4>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    uint64_t need = (a.n_nodes + 32 * warps - 1) / (32 * warps);
+    uint64_t grid = (uint64_t)per_sm * num_sms;
+    if (grid > need) grid = need;
+    kern<<<(unsigned)grid, warps * 32, smem, st>>>(a, lay.p2, lay.bytes);
+    return cudaGetLastError();
+}
+
+}  // namespace vann

@@ -1,0 +1,282 @@
+"""Python host mirror of the B200-native Vamana / FreshVamana engine.
+
+Thin ctypes layer over libvann.so (the C ABI in include/vann.h).  Device
+memory and streams come from torch; every computation runs in the library's
+CUDA kernels.  There is no CPU fallback: importing this module on a machine
+without the built library raises.
+
+Two layers:
+  * ``Index``   -- one vann_index handle, pythonic names.
+  * ``Vamana``  -- the reference's class interface (vamana/include/vamana.cuh:36-146):
+                   searchPoints / insertPoints / deletePoints / patchGraph /
+                   saveGraph, with the reference's staging semantics for inserts.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libvann.so")
+
+OK, ERR_INVALID, ERR_CUDA, ERR_CAPACITY, ERR_IO, ERR_HOP_LIMIT = 0, 1, 2, 3, 4, 5
+ERR_NOT_FOUND, ERR_TIMEOUT, ERR_OOM, ERR_UNSUPPORTED, ERR_STATE = 6, 7, 8, 9, 10
+STORE_F32, STORE_BF16, STORE_FP8, STORE_U8 = 0, 1, 2, 3
+STORES = {"f32": STORE_F32, "bf16": STORE_BF16, "fp8": STORE_FP8, "u8": STORE_U8}
+QUIRK_SKIP_BATCH_INDEX = 0x1
+NONE_ID = 0xFFFFFFFF
+
+# every symbol include/vann.h declares
+EXPORTS = [
+    "vann_status_string", "vann_last_error", "vann_abi_version", "vann_create", "vann_destroy",
+    "vann_get_info", "vann_load_graph", "vann_save_graph", "vann_set_graph", "vann_get_graph",
+    "vann_build", "vann_search", "vann_search_stats", "vann_sync", "vann_insert", "vann_delete", "vann_delete_by_vector",
+    "vann_consolidate",
+]
+
+
+class VannError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"vann status {status}: {msg}")
+        self.status = status
+
+
+class Params(C.Structure):
+    _fields_ = [("dim", C.c_uint32), ("degree", C.c_uint32), ("build_L", C.c_uint32),
+                ("alpha", C.c_float), ("capacity", C.c_uint64), ("max_visited", C.c_uint32),
+                ("max_reverse", C.c_uint32), ("flags", C.c_uint32), ("stores", C.c_uint32)]
+
+
+class SearchParams(C.Structure):
+    _fields_ = [("L", C.c_uint32), ("k", C.c_uint32), ("store", C.c_uint32), ("rerank", C.c_uint32),
+                ("flags", C.c_uint32), ("max_hops", C.c_uint32)]
+
+
+class Info(C.Structure):
+    _fields_ = [("size", C.c_uint64), ("capacity", C.c_uint64), ("live", C.c_uint64),
+                ("free_ids", C.c_uint64), ("entry", C.c_uint32), ("dim", C.c_uint32),
+                ("degree", C.c_uint32), ("consistent", C.c_uint32), ("device_bytes", C.c_uint64)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libvann.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run cs5013-project_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        vp, u64, u32 = C.c_void_p, C.c_uint64, C.c_uint32
+        sig = {
+            "vann_status_string": (C.c_char_p, [C.c_int]),
+            "vann_last_error": (C.c_char_p, []),
+            "vann_abi_version": (C.c_int, []),
+            "vann_create": (C.c_int, [C.POINTER(Params), C.POINTER(vp)]),
+            "vann_destroy": (C.c_int, [vp]),
+            "vann_get_info": (C.c_int, [vp, C.POINTER(Info)]),
+            "vann_load_graph": (C.c_int, [vp, C.c_char_p, u64, u32]),
+            "vann_save_graph": (C.c_int, [vp, C.c_char_p]),
+            "vann_set_graph": (C.c_int, [vp, vp, vp, vp, u64, u32, u32]),
+            "vann_get_graph": (C.c_int, [vp, vp, vp, vp]),
+            "vann_build": (C.c_int, [vp, vp, u64, u64, u64, u32, vp]),
+            "vann_search": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp, vp]),
+            "vann_search_stats": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp, vp, vp, vp, vp]),
+            "vann_sync": (C.c_int, [vp, vp]),
+            "vann_insert": (C.c_int, [vp, vp, u64, vp, vp]),
+            "vann_delete": (C.c_int, [vp, vp, u64, vp]),
+            "vann_delete_by_vector": (C.c_int, [vp, vp, u64, vp, vp]),
+            "vann_consolidate": (C.c_int, [vp, vp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(st: int):
+    if st != OK:
+        raise VannError(st, lib().vann_last_error().decode())
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_ptr(stream):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _dev(t, dtype):
+    torch = _torch()
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == dtype and t.is_contiguous()):
+        raise TypeError(f"expected a contiguous CUDA tensor of {dtype}")
+    return C.c_void_p(t.data_ptr())
+
+
+class Index:
+    """One device-resident Vamana index (vann_index)."""
+
+    def __init__(self, dim: int, degree: int = 64, build_L: int = 100, alpha: float = 1.2,
+                 capacity: int = 1 << 20, max_visited: int = 600, max_reverse: int = 500,
+                 quirks: int = 0, stores=("f32",)):
+        mask = 0
+        for s in stores:
+            if s != "f32":
+                mask |= 1 << STORES[s]
+        p = Params(dim, degree, build_L, alpha, capacity, max_visited, max_reverse, quirks, mask)
+        h = C.c_void_p()
+        _check(lib().vann_create(C.byref(p), C.byref(h)))
+        self._h = h
+        self.dim, self.degree = dim, degree
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().vann_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------------- graph I/O
+    def info(self) -> dict:
+        i = Info()
+        _check(lib().vann_get_info(self._h, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in Info._fields_}
+
+    def set_graph(self, vecs, deg, adj, entry: int, consistent: bool = False):
+        import numpy as np
+        vecs = np.ascontiguousarray(vecs, dtype=np.float32)
+        deg = np.ascontiguousarray(deg, dtype=np.uint32)
+        adj = np.ascontiguousarray(adj, dtype=np.uint32)
+        assert adj.shape[1] == self.degree and vecs.shape[1] == self.dim
+        _check(lib().vann_set_graph(self._h, vecs.ctypes.data, deg.ctypes.data, adj.ctypes.data,
+                                    vecs.shape[0], entry, int(consistent)))
+
+    def get_graph(self):
+        import numpy as np
+        n = self.info()["size"]
+        vecs = np.empty((n, self.dim), np.float32)
+        deg = np.empty(n, np.uint32)
+        adj = np.empty((n, self.degree), np.uint32)
+        _check(lib().vann_get_graph(self._h, vecs.ctypes.data, deg.ctypes.data, adj.ctypes.data))
+        return vecs, deg, adj
+
+    def load_graph(self, path: str, n: int, entry: int):
+        _check(lib().vann_load_graph(self._h, path.encode(), n, entry))
+
+    def save_graph(self, path: str):
+        _check(lib().vann_save_graph(self._h, path.encode()))
+
+    # ---------------------------------------------------------------- hot path
+    def build(self, vecs, batch: int = 0, seed: int = 0, entry: int | None = None, stream=None):
+        torch = _torch()
+        _check(lib().vann_build(self._h, _dev(vecs, torch.float32), vecs.shape[0], batch, seed,
+                                NONE_ID if entry is None else entry, _stream_ptr(stream)))
+
+    def search(self, queries, k: int, L: int, store: str = "f32", rerank: bool = False,
+               quirks: int = 0, max_hops: int = 0, out=None, stream=None):
+        torch = _torch()
+        nq = queries.shape[0]
+        if out is None:
+            ids = torch.empty((nq, k), dtype=torch.int32, device=queries.device)
+            dists = torch.empty((nq, k), dtype=torch.float32, device=queries.device)
+        else:
+            ids, dists = out
+        sp = SearchParams(L, k, STORES[store], int(rerank), quirks, max_hops)
+        _check(lib().vann_search(self._h, _dev(queries, torch.float32), nq, C.byref(sp),
+                                 _dev(ids, torch.int32), _dev(dists, torch.float32), _stream_ptr(stream)))
+        return ids, dists
+
+    def search_stats(self, queries, k: int, L: int, store: str = "f32", rerank: bool = False,
+                     quirks: int = 0, max_hops: int = 0, stream=None):
+        """search() plus per-query (hops, distance evaluations, adjacency words)."""
+        torch = _torch()
+        nq = queries.shape[0]
+        ids = torch.empty((nq, k), dtype=torch.int32, device=queries.device)
+        dists = torch.empty((nq, k), dtype=torch.float32, device=queries.device)
+        st = torch.empty((3, nq), dtype=torch.int32, device=queries.device)
+        sp = SearchParams(L, k, STORES[store], int(rerank), quirks, max_hops)
+        _check(lib().vann_search_stats(self._h, _dev(queries, torch.float32), nq, C.byref(sp),
+                                       _dev(ids, torch.int32), _dev(dists, torch.float32),
+                                       C.c_void_p(st[0].data_ptr()), C.c_void_p(st[1].data_ptr()),
+                                       C.c_void_p(st[2].data_ptr()), _stream_ptr(stream)))
+        return ids, dists, st
+
+    def sync(self, stream=None):
+        _check(lib().vann_sync(self._h, _stream_ptr(stream)))
+
+    def insert(self, vecs, stream=None):
+        torch = _torch()
+        ids = torch.empty(vecs.shape[0], dtype=torch.int32, device=vecs.device)
+        _check(lib().vann_insert(self._h, _dev(vecs, torch.float32), vecs.shape[0], _dev(ids, torch.int32),
+                                 _stream_ptr(stream)))
+        return ids
+
+    def delete(self, ids, stream=None):
+        torch = _torch()
+        _check(lib().vann_delete(self._h, _dev(ids, torch.int32), ids.shape[0], _stream_ptr(stream)))
+
+    def delete_by_vector(self, vecs, stream=None):
+        torch = _torch()
+        out = torch.empty(vecs.shape[0], dtype=torch.int32, device=vecs.device)
+        st = lib().vann_delete_by_vector(self._h, _dev(vecs, torch.float32), vecs.shape[0],
+                                         _dev(out, torch.int32), _stream_ptr(stream))
+        if st not in (OK, ERR_NOT_FOUND):
+            _check(st)
+        return out
+
+    def consolidate(self, stream=None):
+        _check(lib().vann_consolidate(self._h, _stream_ptr(stream)))
+
+
+class Vamana:
+    """The reference's index class (vamana/include/vamana.cuh:36-146) on top of Index.
+
+    ``Vamana(vecs, R, L, alpha, ...)`` builds like the reference constructor
+    (vamana_impl.cuh:10-20 -> runVamana :289-360).  insertPoints stages vectors
+    like the reference's InsertList (vamana_impl.cuh:22-33); patchGraph inserts
+    the staged batch and consolidates deletes (:182-265); deletePoints matches
+    by vector (:35-53); searchPoints returns the n x L worklist ids (:55-96).
+    """
+
+    def __init__(self, vecs, R: int = 64, L: int = 199, alpha: float = 1.5, capacity: int | None = None,
+                 entry: int | None = None, seed: int = 0, reference_quirks: bool = True,
+                 max_visited: int = 600, max_reverse: int = 500):
+        self.R, self.L = R, L
+        n = vecs.shape[0]
+        self.quirks = QUIRK_SKIP_BATCH_INDEX if reference_quirks else 0
+        self.index = Index(vecs.shape[1], R, L, alpha, capacity or max(int(n * 1.3), n + 1), max_visited,
+                           max_reverse, self.quirks)
+        self.index.build(vecs, batch=0, seed=seed, entry=entry)
+        self._staged = []
+
+    def insertPoints(self, d_vecs, num: int | None = None):
+        self._staged.append(d_vecs[: num if num is not None else d_vecs.shape[0]].contiguous())
+
+    def deletePoints(self, d_vecs, num: int | None = None):
+        return self.index.delete_by_vector(d_vecs[: num if num is not None else d_vecs.shape[0]].contiguous())
+
+    def searchPoints(self, d_q, num: int | None = None):
+        q = d_q[: num if num is not None else d_q.shape[0]].contiguous()
+        ids, _ = self.index.search(q, k=self.L, L=self.L, quirks=self.quirks)
+        return ids
+
+    def patchGraph(self):
+        torch = _torch()
+        if self._staged:
+            self.index.insert(torch.cat(self._staged, 0).contiguous())
+            self._staged = []
+        self.index.consolidate()
+
+    def saveGraph(self, path: str):
+        self.index.save_graph(path)

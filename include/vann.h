@@ -1,0 +1,162 @@
+/*
+ * vann.h -- C ABI of the B200-native Vamana / FreshVamana engine (libvann.so).
+ *
+ * Every entry point takes plain pointers and sizes, returns a vann_status and
+ * never exits the process.  Device pointers are caller-owned CUDA device memory
+ * on the current device; `stream` is a cudaStream_t passed as void* (NULL = the
+ * legacy default stream).  One vann_index is externally synchronised: do not
+ * call into the same handle from two host threads at once.
+ *
+ * The reference interface each entry point replaces is cited beside it
+ * (paths relative to the reference project, VishankSingh/CS5013-Project).
+ */
+#ifndef VANN_H
+#define VANN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VANN_ABI_VERSION 1
+
+typedef enum {
+    VANN_OK              = 0,
+    VANN_ERR_INVALID     = 1,  /* bad argument */
+    VANN_ERR_CUDA        = 2,  /* a CUDA runtime call failed (see vann_last_error) */
+    VANN_ERR_CAPACITY    = 3,  /* index capacity exhausted */
+    VANN_ERR_IO          = 4,  /* file could not be read or written */
+    VANN_ERR_HOP_LIMIT   = 5,  /* a search stopped at max_hops (results are still written) */
+    VANN_ERR_NOT_FOUND   = 6,  /* delete-by-vector found no matching node */
+    VANN_ERR_TIMEOUT     = 7,  /* a bounded device wait gave up */
+    VANN_ERR_OOM         = 8,  /* device allocation failed */
+    VANN_ERR_UNSUPPORTED = 9,  /* combination not built (e.g. dim not a multiple of 4) */
+    VANN_ERR_STATE       = 10  /* call not valid in the index's current state */
+} vann_status;
+
+/* Storage forms of the base vectors.  F32 is always kept (exact distances,
+ * pruning, rerank); the others are extra traversal copies. */
+typedef enum {
+    VANN_STORE_F32  = 0,
+    VANN_STORE_BF16 = 1, /* round-to-nearest-even bf16, FP32 accumulation */
+    VANN_STORE_FP8  = 2, /* e4m3 with one FP32 scale per vector (amax / 448) */
+    VANN_STORE_U8   = 3  /* uint8 codes; exact for integer data in [0, 255] */
+} vann_store;
+
+/* Reference quirks, reproduced for parity when set. */
+#define VANN_QUIRK_SKIP_BATCH_INDEX 0x1u /* skip neighbour id == query's batch index
+                                            (vamana/include/search.cuh:126) */
+
+typedef struct {
+    uint32_t dim;         /* D; must be a multiple of 4, <= 512 */
+    uint32_t degree;      /* R (max out-degree), <= 128 */
+    uint32_t build_L;     /* worklist size used by build / insert searches */
+    float    alpha;       /* RobustPrune alpha (reference hard-codes 1.5,
+                             vamana/include/vamana_impl.cuh:297) */
+    uint64_t capacity;    /* max number of nodes the index can hold */
+    uint32_t max_visited; /* expansion-list cap per build search (reference 600,
+                             vamana/include/constants.cuh:13) */
+    uint32_t max_reverse; /* reverse-candidate cap per node (reference 500,
+                             vamana/include/constants.cuh:20) */
+    uint32_t flags;       /* VANN_QUIRK_* applied to build / insert searches */
+    uint32_t stores;      /* bitmask (1 << vann_store) of extra traversal copies */
+} vann_params;
+
+typedef struct {
+    uint32_t L;        /* worklist size, >= k, <= 1024 */
+    uint32_t k;        /* results per query */
+    uint32_t store;    /* vann_store the traversal reads */
+    uint32_t rerank;   /* 1: exact FP32 rerank of the final worklist before top-k */
+    uint32_t flags;    /* VANN_QUIRK_* */
+    uint32_t max_hops; /* 0 = default (1,000,000) */
+} vann_search_params;
+
+typedef struct {
+    uint64_t size;         /* node ids in use (0 .. size-1, some may be deleted) */
+    uint64_t capacity;
+    uint64_t live;         /* size minus deleted */
+    uint64_t free_ids;     /* consolidated ids waiting for reuse */
+    uint32_t entry;        /* search entry point */
+    uint32_t dim, degree;
+    uint32_t consistent;   /* 1 when every adjacency list came from RobustPrune with alpha */
+    uint64_t device_bytes; /* device memory held by the index */
+} vann_info;
+
+typedef struct vann_index vann_index;
+
+const char* vann_status_string(vann_status s);
+/* Message of the last failing call on this host thread ("" if none). */
+const char* vann_last_error(void);
+int         vann_abi_version(void);
+
+/* Vamana<T>::Vamana storage + GraphT (vamana/include/vamana.cuh:36-146,
+ * graphT.cuh:56-59).  Allocates capacity on the current device. */
+vann_status vann_create(const vann_params* params, vann_index** out);
+vann_status vann_destroy(vann_index* index);
+vann_status vann_get_info(const vann_index* index, vann_info* out);
+
+/* initGraph (vamana/include/utils.cuh:113-148): read n records of
+ * {float vec[D]; uint32 deg; uint32 nbr[R]} (772 bytes at D=128, R=64). */
+vann_status vann_load_graph(vann_index* index, const char* path, uint64_t n, uint32_t entry);
+/* saveGraph (vamana.cu:1346-1362): write size records in the same layout. */
+vann_status vann_save_graph(vann_index* index, const char* path);
+
+/* Host-array graph upload / download (test and interop path).  consistent=1
+ * asserts that every list came from RobustPrune with this index's alpha. */
+vann_status vann_set_graph(vann_index* index, const float* h_vecs, const uint32_t* h_deg,
+                           const uint32_t* h_adj, uint64_t n, uint32_t entry, uint32_t consistent);
+vann_status vann_get_graph(vann_index* index, float* h_vecs, uint32_t* h_deg, uint32_t* h_adj);
+
+/* Vamana<T>::Vamana -> runVamana (vamana/include/vamana_impl.cuh:10-20,289-360).
+ * Builds over n device vectors.  batch >= n: one batch over a seeded random
+ * R-regular start graph (the reference build).  batch < n: that build on the
+ * first batch, then batched inserts of `batch` nodes.  entry = UINT32_MAX picks
+ * the medoid (argmin distance to the centroid) of the first batch.
+ * Synchronises `stream` before returning. */
+vann_status vann_build(vann_index* index, const float* d_vecs, uint64_t n, uint64_t batch,
+                       uint64_t seed, uint32_t entry, void* stream);
+
+/* Vamana<T>::searchPoints (vamana/include/vamana_impl.cuh:55-96, GreedySearch
+ * search.cuh:226-367).  d_queries: nq x dim FP32.  Writes nq x k ids / squared
+ * L2 distances, padded with UINT32_MAX / +inf.  Asynchronous on `stream`. */
+vann_status vann_search(vann_index* index, const float* d_queries, uint64_t nq,
+                        const vann_search_params* sp, uint32_t* d_ids, float* d_dists,
+                        void* stream);
+/* vann_search plus per-query work counters (device arrays of nq, any may be
+ * NULL): expansions (hops), distance evaluations, adjacency words read. */
+vann_status vann_search_stats(vann_index* index, const float* d_queries, uint64_t nq,
+                              const vann_search_params* sp, uint32_t* d_ids, float* d_dists,
+                              uint32_t* d_hops, uint32_t* d_evals, uint32_t* d_adj_words,
+                              void* stream);
+/* Device status word of earlier asynchronous calls: synchronises `stream`,
+ * returns VANN_ERR_HOP_LIMIT if a search hit its hop cap since the last call,
+ * and clears it. */
+vann_status vann_sync(vann_index* index, void* stream);
+
+/* Vamana<T>::insertPoints + patchGraph (vamana_impl.cuh:22-33,182-265):
+ * inserts n device vectors as one batch (search, RobustPrune, reverse edges,
+ * re-prune of the touched nodes).  New ids (reused consolidated ids first,
+ * then appended) go to d_ids_out (may be NULL).  Synchronises `stream`. */
+vann_status vann_insert(vann_index* index, const float* d_vecs, uint64_t n, uint32_t* d_ids_out,
+                        void* stream);
+
+/* Vamana<T>::deletePoints (vamana_impl.cuh:35-53) by id: lazy tombstones that
+ * searches skip (delete_list.cuh:109-115).  Asynchronous. */
+vann_status vann_delete(vann_index* index, const uint32_t* d_ids, uint64_t n, void* stream);
+/* deletePoints by exact vector match (findPointsKernel, kernels.cuh:905-933).
+ * d_ids_out[i] = matched id or -1.  Synchronises `stream`. */
+vann_status vann_delete_by_vector(vann_index* index, const float* d_vecs, uint64_t n,
+                                  int32_t* d_ids_out, void* stream);
+
+/* Vamana<T>::patchGraph (vamana_impl.cuh:182-265) extended with FreshVamana
+ * delete consolidation: every live node that points at a deleted node is
+ * re-pruned over its live out-neighbours plus the deleted nodes' live
+ * out-neighbours; deleted ids are then freed for reuse.  Synchronises. */
+vann_status vann_consolidate(vann_index* index, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,193 @@
+"""ctypes wrapper over oracle/liboracle.so -- the CPU parity checker.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / --impl reference legs of bench.py.  The product never imports it.
+The C restatement it wraps cites the reference file:line for every step
+(oracle/vann_oracle.c).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+BLOOM_CHUNK32, BLOOM_SEQUENTIAL, BLOOM_SNAPSHOT = 0, 1, 2
+NONE = 0xFFFFFFFF
+
+
+class _Graph(C.Structure):
+    _fields_ = [
+        ("vecs", C.c_void_p),
+        ("n", C.c_int64),
+        ("dim", C.c_int32),
+        ("deg", C.c_void_p),
+        ("adj", C.c_void_p),
+        ("R", C.c_int32),
+        ("tomb", C.c_void_p),
+    ]
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return os.path.join(_HERE, "liboracle.so")
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        L.vo_bf_h1.restype = C.c_uint32
+        L.vo_bf_h1.argtypes = [C.c_uint32]
+        L.vo_bf_h2.restype = C.c_uint32
+        L.vo_bf_h2.argtypes = [C.c_uint32]
+        L.vo_medoid.restype = C.c_int64
+        L.vo_medoid.argtypes = [C.c_void_p, C.c_int64, C.c_int]
+        L.vo_search_batch.restype = C.c_int
+        L.vo_search_batch.argtypes = [C.POINTER(_Graph), C.c_void_p, C.c_int64, C.c_int, C.c_int,
+                                      C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_int]
+        L.vo_search_one.restype = C.c_int
+        L.vo_search_one.argtypes = [C.POINTER(_Graph), C.c_void_p, C.c_int, C.c_uint32, C.c_uint32,
+                                    C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.vo_robust_prune.restype = C.c_int
+        L.vo_robust_prune.argtypes = [C.POINTER(_Graph), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                      C.c_float, C.c_int, C.c_void_p, C.c_void_p]
+        L.vo_vamana_batch.restype = C.c_int
+        L.vo_vamana_batch.argtypes = [C.POINTER(_Graph), C.c_int64, C.c_int64, C.c_int, C.c_float,
+                                      C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.vo_random_graph.restype = None
+        L.vo_random_graph.argtypes = [C.c_int64, C.c_int, C.c_uint64, C.c_void_p, C.c_void_p]
+        L.vo_bruteforce_knn.restype = None
+        L.vo_bruteforce_knn.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, C.c_int,
+                                        C.c_void_p, C.c_void_p, C.c_int]
+        _LIB = L
+    return _LIB
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+class Graph:
+    """Host copy of an index: vectors, degrees, adjacency (n x R), tombstones."""
+
+    def __init__(self, vecs: np.ndarray, deg: np.ndarray, adj: np.ndarray, tomb: np.ndarray | None = None):
+        self.vecs = np.ascontiguousarray(vecs, dtype=np.float32)
+        self.deg = np.ascontiguousarray(deg, dtype=np.uint32)
+        self.adj = np.ascontiguousarray(adj, dtype=np.uint32)
+        self.tomb = None if tomb is None else np.ascontiguousarray(tomb, dtype=np.uint32)
+
+    @property
+    def n(self):
+        return self.vecs.shape[0]
+
+    @property
+    def R(self):
+        return self.adj.shape[1]
+
+    def _c(self):
+        return _Graph(_p(self.vecs), self.n, self.vecs.shape[1], _p(self.deg), _p(self.adj), self.R,
+                      _p(self.tomb))
+
+    def search(self, q, L, k, entry, skip_mode=0, bloom_mode=BLOOM_CHUNK32, max_hops=1 << 30, threads=0):
+        q = np.ascontiguousarray(q, dtype=np.float32)
+        nq = q.shape[0]
+        ids = np.empty((nq, k), np.uint32)
+        d = np.empty((nq, k), np.float32)
+        hops = np.empty(nq, np.int32)
+        evals = np.empty(nq, np.int64)
+        g = self._c()
+        st = lib().vo_search_batch(C.byref(g), _p(q), nq, L, k, entry, skip_mode, bloom_mode, max_hops,
+                                   _p(ids), _p(d), _p(hops), _p(evals), threads)
+        return st, ids, d, hops, evals
+
+    def search_one(self, q, L, entry, skip_id=NONE, bloom_mode=BLOOM_CHUNK32, max_visited=600,
+                   max_hops=1 << 30):
+        q = np.ascontiguousarray(q, dtype=np.float32)
+        wi = np.empty(L, np.uint32)
+        wd = np.empty(L, np.float32)
+        wn = C.c_int(0)
+        vi = np.empty(max_visited, np.uint32)
+        vd = np.empty(max_visited, np.float32)
+        vn = C.c_int(0)
+        hops = C.c_int(0)
+        ev = C.c_int64(0)
+        g = self._c()
+        st = lib().vo_search_one(C.byref(g), _p(q), L, entry, skip_id, bloom_mode, max_visited, max_hops,
+                                 _p(wi), _p(wd), C.byref(wn), _p(vi), _p(vd), C.byref(vn), C.byref(hops),
+                                 C.byref(ev))
+        return st, wi[: wn.value], wd[: wn.value], vi[: vn.value], vd[: vn.value], hops.value, ev.value
+
+    def robust_prune(self, node_vec, cand, cand_d, alpha, R):
+        cand = np.ascontiguousarray(cand, dtype=np.uint32)
+        cand_d = np.ascontiguousarray(cand_d, dtype=np.float32)
+        out = np.empty(R, np.uint32)
+        g = self._c()
+        nv = np.ascontiguousarray(node_vec, dtype=np.float32)
+        d = lib().vo_robust_prune(C.byref(g), _p(nv), _p(cand), _p(cand_d), len(cand), alpha, R, _p(out), None)
+        return out[:d]
+
+    def vamana_batch(self, batch_start, batch_n, L, alpha, entry, max_visited=600, max_reverse=500,
+                     skip_mode=1, bloom_mode=BLOOM_CHUNK32, threads=0):
+        g = self._c()
+        return lib().vo_vamana_batch(C.byref(g), batch_start, batch_n, L, alpha, entry, max_visited,
+                                     max_reverse, skip_mode, bloom_mode, threads)
+
+
+def bf_h1(x: int) -> int:
+    return lib().vo_bf_h1(x)
+
+
+def bf_h2(x: int) -> int:
+    return lib().vo_bf_h2(x)
+
+
+def random_graph(n: int, R: int, seed: int):
+    deg = np.empty(n, np.uint32)
+    adj = np.empty((n, R), np.uint32)
+    lib().vo_random_graph(n, R, seed, _p(deg), _p(adj))
+    return deg, adj
+
+
+def medoid(vecs: np.ndarray) -> int:
+    v = np.ascontiguousarray(vecs, dtype=np.float32)
+    return int(lib().vo_medoid(_p(v), v.shape[0], v.shape[1]))
+
+
+def bruteforce_knn(base: np.ndarray, q: np.ndarray, k: int, threads: int = 0):
+    base = np.ascontiguousarray(base, dtype=np.float32)
+    q = np.ascontiguousarray(q, dtype=np.float32)
+    ids = np.empty((q.shape[0], k), np.uint32)
+    d = np.empty((q.shape[0], k), np.float64)
+    lib().vo_bruteforce_knn(_p(base), base.shape[0], _p(q), q.shape[0], base.shape[1], k, _p(ids), _p(d), threads)
+    return ids, d
+
+
+def build_index(vecs, R, L, alpha, entry=None, seed=0, skip_mode=1, bloom_mode=BLOOM_CHUNK32,
+                max_visited=600, max_reverse=500, threads=0):
+    """Reference build (vamana_impl.cuh:289-360 runVamana): one batch of all nodes
+    over a seeded random R-regular start graph."""
+    n = vecs.shape[0]
+    deg, adj = random_graph(n, R, seed)
+    g = Graph(vecs, deg, adj)
+    if entry is None:
+        entry = medoid(vecs)
+    st = g.vamana_batch(0, n, L, alpha, entry, max_visited, max_reverse, skip_mode, bloom_mode, threads)
+    assert st == 0, st
+    return g, entry
+
+
+def recall_at_k(found: np.ndarray, truth: np.ndarray, k: int) -> float:
+    hit = 0
+    for f, t in zip(found[:, :k], truth[:, :k]):
+        hit += len(set(f.tolist()) & set(t.tolist()))
+    return hit / (truth.shape[0] * k)

@@ -1,0 +1,100 @@
+/*
+ * vann_oracle.h -- CPU restatement of the reference's Vamana / FreshVamana hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the parity checker for the CUDA
+ * product in cs5013-project_b200/.  Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / --impl reference legs of bench.py may load it.  The product
+ * never calls it and has no CPU fallback.
+ *
+ * Each function cites the reference code it restates (paths relative to the
+ * reference project root).  Where the reference is non-deterministic (atomic
+ * arrival order, racy bloom-filter check-then-set), the oracle fixes one member
+ * of the reference's allowed behaviour set and the CUDA kernels implement the
+ * same member:
+ *   - bloom filter: adjacency slots are processed in chunks of 32 in adjacency
+ *     order; every slot of a chunk is checked against the filter as it stood
+ *     before the chunk, then the chunk's new neighbours are marked.  This is
+ *     what one convergent warp of filterNeighbors (vamana/include/search.cuh:119-137)
+ *     does.  VO_BLOOM_SEQUENTIAL (chunk 1) and VO_BLOOM_SNAPSHOT (whole list)
+ *     are the two other members, kept for the golden-graph experiment.
+ *   - new neighbours of one expansion with equal distance are ordered by node id
+ *     (the reference orders them by atomicAdd arrival, search.cuh:134).
+ *   - reverse-index entries arrive in ascending source-node order, each source's
+ *     entries in RobustPrune selection order (kernels.cuh:293-301 uses atomics).
+ */
+#ifndef VANN_ORACLE_H
+#define VANN_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VO_BF_ENTRIES 39988u /* vamana/include/bloom_filter.cuh:7 */
+#define VO_NONE 0xFFFFFFFFu
+
+enum { VO_BLOOM_CHUNK32 = 0, VO_BLOOM_SEQUENTIAL = 1, VO_BLOOM_SNAPSHOT = 2 };
+
+/* status codes (match include/vann.h) */
+enum { VO_OK = 0, VO_ERR_INVALID = 1, VO_ERR_HOP_LIMIT = 5 };
+
+typedef struct {
+    const float*    vecs;  /* n x dim, row-major */
+    int64_t         n;
+    int32_t         dim;
+    uint32_t*       deg;   /* n */
+    uint32_t*       adj;   /* n x R */
+    int32_t         R;
+    const uint32_t* tomb;  /* bitmap of deleted ids (bit i of word i>>5), may be NULL */
+} vo_graph;
+
+uint32_t vo_bf_h1(uint32_t x);
+uint32_t vo_bf_h2(uint32_t x);
+float    vo_l2sq(const float* a, const float* b, int dim);
+
+/* One GreedySearch (vamana/include/search.cuh:20-367).
+ * Outputs the final worklist (<= L entries, sorted) and the expansion list
+ * (parents in expansion order, capped at max_visited) with their distances. */
+int vo_search_one(const vo_graph* g, const float* q, int L, uint32_t entry, uint32_t skip_id,
+                  int bloom_mode, int max_visited, int max_hops, uint32_t* wl_ids, float* wl_d,
+                  int* wl_n, uint32_t* vis_ids, float* vis_d, int* vis_n, int* hops,
+                  int64_t* evals);
+
+/* Batched search: out_ids/out_d are n x k (padded with VO_NONE / +inf).
+ * skip_mode: 0 = no skip, 1 = skip the query's batch index (reference quirk
+ * search.cuh:126).  hops/evals may be NULL.  threads <= 0 means all cores. */
+int vo_search_batch(const vo_graph* g, const float* q, int64_t nq, int L, int k, uint32_t entry,
+                    int skip_mode, int bloom_mode, int max_hops, uint32_t* out_ids, float* out_d,
+                    int32_t* hops, int64_t* evals, int threads);
+
+/* RobustPrune over a sorted candidate list (kernels.cuh:232-356).  Returns the
+ * new degree; writes the chosen ids in selection order to out. */
+int vo_robust_prune(const vo_graph* g, const float* node_vec, const uint32_t* cand,
+                    const float* cand_d, int nc, float alpha, int R, uint32_t* out,
+                    int64_t* evals);
+
+/* One Vamana batch (vamana_impl.cuh:289-360 runVamana / :182-265 patchGraph):
+ * search every batch node from `entry`, RobustPrune its out-neighbours,
+ * record reverse edges, then re-prune every node 0..n-1 over reverse u out.
+ * Batch nodes are ids batch_start .. batch_start+batch_n-1 and their vectors are
+ * g->vecs rows.  skip_mode: 0 none, 1 batch index (reference), 2 node id.
+ * g->deg / g->adj are updated in place. */
+int vo_vamana_batch(vo_graph* g, int64_t batch_start, int64_t batch_n, int L, float alpha,
+                    uint32_t entry, int max_visited, int max_reverse, int skip_mode,
+                    int bloom_mode, int threads);
+
+/* Deterministic random initial graph (hash-based, no self loops). */
+void vo_random_graph(int64_t n, int R, uint64_t seed, uint32_t* deg, uint32_t* adj);
+
+/* argmin_i ||x_i - mean||^2 in FP64 (parth/tools/vamana.py:25-29). */
+int64_t vo_medoid(const float* vecs, int64_t n, int dim);
+
+/* Exact kNN in FP64 (ties by id). */
+void vo_bruteforce_knn(const float* base, int64_t n, const float* q, int64_t nq, int dim, int k,
+                       uint32_t* out_ids, double* out_d, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

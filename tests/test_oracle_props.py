@@ -1,0 +1,97 @@
+"""Properties of the CPU oracle on seeded synthetic data (no GPU, no reference files)."""
+import numpy as np
+import pytest
+
+from vann import workload
+
+
+@pytest.fixture(scope="module")
+def small():
+    base = workload.mixture(3000, 128, 30, seed=11)
+    q = workload.mixture(50, 128, 30, seed=12)
+    return base, q
+
+
+def test_build_degrees_and_ids(oracle, small):
+    base, _ = small
+    g, entry = oracle.build_index(base, R=32, L=75, alpha=1.2, seed=5)
+    assert g.deg.max() <= 32 and g.deg.min() >= 1
+    for i in range(0, g.n, 97):
+        row = g.adj[i, :g.deg[i]]
+        assert (row < g.n).all()
+        assert len(set(row.tolist())) == len(row)  # RobustPrune never keeps duplicates
+
+
+def test_build_is_deterministic(oracle, small):
+    base, _ = small
+    a, _ = oracle.build_index(base, R=32, L=50, alpha=1.2, seed=5, threads=1)
+    b, _ = oracle.build_index(base, R=32, L=50, alpha=1.2, seed=5, threads=8)
+    assert np.array_equal(a.deg, b.deg)
+    for i in range(a.n):
+        assert np.array_equal(a.adj[i, :a.deg[i]], b.adj[i, :b.deg[i]])
+
+
+def test_recall(oracle, small):
+    base, q = small
+    g, entry = oracle.build_index(base, R=32, L=75, alpha=1.2, seed=5)
+    st, ids, d, hops, evals = g.search(q, 75, 10, entry)
+    truth, td = oracle.bruteforce_knn(base, q, 10)
+    assert st == 0
+    assert oracle.recall_at_k(ids, truth, 10) >= 0.95
+    # reported distances are the exact squared L2 of the reported ids
+    for s in range(5):
+        for t in range(10):
+            exact = float(((base[ids[s, t]].astype(np.float64) - q[s]) ** 2).sum())
+            assert d[s, t] == pytest.approx(exact, rel=0, abs=0)
+
+
+def test_robust_prune_rule(oracle, small):
+    base, _ = small
+    g = oracle.Graph(base, np.zeros(len(base), np.uint32), np.zeros((len(base), 32), np.uint32))
+    node = 7
+    cand = np.array([i for i in range(100) if i != node], np.uint32)
+    cd = np.array([((base[c] - base[node]) ** 2).sum() for c in cand], np.float32)
+    order = np.argsort(cd, kind="stable")
+    cand, cd = cand[order], cd[order]
+    out = g.robust_prune(base[node], cand, cd, 1.2, 32)
+    # restate the rule directly
+    status = np.zeros(len(cand), int)
+    chosen = []
+    while len(chosen) < 32:
+        idx = np.where(status == 0)[0]
+        if len(idx) == 0:
+            break
+        f = idx[0]
+        chosen.append(cand[f])
+        status[f] = 2
+        ps = base[cand[f]]
+        for t in np.where(status == 0)[0]:
+            dd = np.float32(((base[cand[t]] - ps) ** 2).sum())
+            if np.float32(dd * np.float32(1.2)) <= cd[t]:
+                status[t] = 1
+    assert out.tolist() == [int(c) for c in chosen]
+
+
+def test_hop_limit_status(oracle, small):
+    base, q = small
+    g, entry = oracle.build_index(base, R=32, L=50, alpha=1.2, seed=5)
+    st, ids, d, hops, evals = g.search(q[:4], 50, 10, entry, max_hops=3)
+    assert st == 5 and (hops <= 3).all()
+
+
+def test_insert_batch_matches_full_rebuild_shape(oracle, small):
+    base, q = small
+    n0 = 2000
+    deg, adj = oracle.random_graph(n0, 32, 9)
+    deg_all = np.zeros(len(base), np.uint32)
+    adj_all = np.zeros((len(base), 32), np.uint32)
+    deg_all[:n0] = deg
+    adj_all[:n0] = adj
+    g = oracle.Graph(base, deg_all, adj_all)
+    entry = oracle.medoid(base[:n0])
+    assert g.vamana_batch(0, n0, 64, 1.2, entry, skip_mode=2) == 0
+    assert g.vamana_batch(n0, 1000, 64, 1.2, entry, skip_mode=0) == 0
+    assert (g.deg[n0:] > 0).all()
+    st, ids, d, _, _ = g.search(q, 64, 10, entry)
+    truth, _ = oracle.bruteforce_knn(base, q, 10)
+    assert oracle.recall_at_k(ids, truth, 10) >= 0.9
