@@ -49,38 +49,51 @@ __device__ __forceinline__ uint32_t bloom_h2(uint32_t x) {
     return (uint32_t)(h % kBloomSlots);
 }
 
+// Both filter slots of one id packed as (h1 << 16) | h2 (each < 39,988 < 2^16).
+// The index keeps this word beside every adjacency entry, so a search reads the
+// slots of a parent's neighbours in the same request as their ids.
+__device__ __forceinline__ uint32_t bloom_pack(uint32_t x) { return (bloom_h1(x) << 16) | bloom_h2(x); }
+
 // ---------------------------------------------------------------- stores
+// Each store reads one 4-element chunk of a row per lane (16, 8 or 4 bytes), so
+// a warp reads a whole 128-dim row in one coalesced request.  kGroup rows are
+// gathered per round (32 registers of raw data per lane whatever the width):
+// narrower elements mean fewer dependent gather rounds per expansion.
 struct StoreF32 {
-    static constexpr int kBytes = 4;
-    __device__ __forceinline__ static float4 load4(const void* base, const float*, uint64_t row,
-                                                   uint32_t D, uint32_t c) {
-        const float4* p = reinterpret_cast<const float4*>(static_cast<const float*>(base) + row * D);
-        return __ldg(p + c);
+    static constexpr int  kGroup  = 8;
+    static constexpr bool kScaled = false;
+    static constexpr bool kBytes8 = false;
+    using raw_t                   = float4;
+    __device__ __forceinline__ static raw_t load(const void* base, uint64_t row, uint32_t D, uint32_t c) {
+        return __ldg(reinterpret_cast<const float4*>(static_cast<const float*>(base) + row * D) + c);
     }
+    __device__ __forceinline__ static raw_t zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+    __device__ __forceinline__ static float4 widen(const raw_t& x, float) { return x; }
 };
 struct StoreBF16 {
-    static constexpr int kBytes = 2;
-    __device__ __forceinline__ static float4 load4(const void* base, const float*, uint64_t row,
-                                                   uint32_t D, uint32_t c) {
-        const uint2* p =
-            reinterpret_cast<const uint2*>(static_cast<const __nv_bfloat16*>(base) + row * D);
-        uint2 u = __ldg(p + c);
-        float4 r;
-        r.x = __uint_as_float(u.x << 16);
-        r.y = __uint_as_float(u.x & 0xffff0000u);
-        r.z = __uint_as_float(u.y << 16);
-        r.w = __uint_as_float(u.y & 0xffff0000u);
-        return r;
+    static constexpr int  kGroup  = 16;
+    static constexpr bool kScaled = false;
+    static constexpr bool kBytes8 = false;
+    using raw_t                   = uint2;
+    __device__ __forceinline__ static raw_t load(const void* base, uint64_t row, uint32_t D, uint32_t c) {
+        return __ldg(reinterpret_cast<const uint2*>(static_cast<const __nv_bfloat16*>(base) + row * D) + c);
+    }
+    __device__ __forceinline__ static raw_t zero() { return make_uint2(0u, 0u); }
+    __device__ __forceinline__ static float4 widen(const raw_t& u, float) {
+        return make_float4(__uint_as_float(u.x << 16), __uint_as_float(u.x & 0xffff0000u),
+                           __uint_as_float(u.y << 16), __uint_as_float(u.y & 0xffff0000u));
     }
 };
 struct StoreFP8 {
-    static constexpr int kBytes = 1;
-    __device__ __forceinline__ static float4 load4(const void* base, const float* scale,
-                                                   uint64_t row, uint32_t D, uint32_t c) {
-        const uint32_t* p =
-            reinterpret_cast<const uint32_t*>(static_cast<const uint8_t*>(base) + row * D);
-        uint32_t u = __ldg(p + c);
-        float    s = __ldg(scale + row);
+    static constexpr int  kGroup  = 16;
+    static constexpr bool kScaled = true;
+    static constexpr bool kBytes8 = false;
+    using raw_t                   = uint32_t;
+    __device__ __forceinline__ static raw_t load(const void* base, uint64_t row, uint32_t D, uint32_t c) {
+        return __ldg(reinterpret_cast<const uint32_t*>(static_cast<const uint8_t*>(base) + row * D) + c);
+    }
+    __device__ __forceinline__ static raw_t zero() { return 0u; }
+    __device__ __forceinline__ static float4 widen(const raw_t& u, float s) {
         __half2_raw lo = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(u & 0xffffu), __NV_E4M3);
         __half2_raw hi = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(u >> 16), __NV_E4M3);
         float2 a = __half22float2(*reinterpret_cast<__half2*>(&lo));
@@ -89,12 +102,15 @@ struct StoreFP8 {
     }
 };
 struct StoreU8 {
-    static constexpr int kBytes = 1;
-    __device__ __forceinline__ static float4 load4(const void* base, const float*, uint64_t row,
-                                                   uint32_t D, uint32_t c) {
-        const uint32_t* p =
-            reinterpret_cast<const uint32_t*>(static_cast<const uint8_t*>(base) + row * D);
-        uint32_t u = __ldg(p + c);
+    static constexpr int  kGroup  = 32;
+    static constexpr bool kScaled = false;
+    static constexpr bool kBytes8 = true;  // exact integer path for integer queries
+    using raw_t                   = uint32_t;
+    __device__ __forceinline__ static raw_t load(const void* base, uint64_t row, uint32_t D, uint32_t c) {
+        return __ldg(reinterpret_cast<const uint32_t*>(static_cast<const uint8_t*>(base) + row * D) + c);
+    }
+    __device__ __forceinline__ static raw_t zero() { return 0u; }
+    __device__ __forceinline__ static float4 widen(const raw_t& u, float) {
         return make_float4((float)(u & 0xffu), (float)((u >> 8) & 0xffu), (float)((u >> 16) & 0xffu),
                            (float)(u >> 24));
     }
@@ -109,86 +125,131 @@ __device__ __forceinline__ float sqdiff4(const float4& q, const float4& x, float
     return acc;
 }
 
-// Reduce 8 per-lane partial sums across the warp in 9 shuffles.  On return the
-// lane holds the full sum of value index vidx(lane) =
-// ((lane>>4)&1)*4 + ((lane>>3)&1)*2 + ((lane>>2)&1); the sum of value j is held
-// by lane vlane(j) = ((j>>2)&1)*16 + ((j>>1)&1)*8 + (j&1)*4.
-__device__ __forceinline__ float transpose_reduce8(const float v[8], uint32_t lane) {
-    float w[4];
+// Register-resident query: FP32 chunks, plus packed uint8 chunks and |q|^2 when
+// every element is an integer in [0, 255] (then uint8 rows use dp4a exactly).
+template <int NCH>
+struct Query {
+    float4   f[NCH];
+    uint32_t u[NCH];
+    int      qq;
+    bool     qint;
+};
+
+template <int NCH>
+__device__ __forceinline__ void load_query(Query<NCH>& q, const float* row, uint32_t D, uint32_t lane) {
+    const uint32_t nchunk = D >> 2;
+    bool           ok     = true;
+    int            qq     = 0;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        bool  up   = lane & 16;
-        float send = up ? v[i] : v[i + 4];
-        float keep = up ? v[i + 4] : v[i];
-        w[i]       = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-    }
-    float x[2];
+    for (int c = 0; c < NCH; ++c) {
+        uint32_t ch = lane + 32u * c;
+        float4   v  = ch < nchunk ? __ldg(reinterpret_cast<const float4*>(row) + ch)
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+        q.f[c]      = v;
+        float e[4]  = {v.x, v.y, v.z, v.w};
+        uint32_t pk = 0;
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
-        bool  up   = lane & 8;
-        float send = up ? w[i] : w[i + 2];
-        float keep = up ? w[i + 2] : w[i];
-        x[i]       = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+        for (int i = 0; i < 4; ++i) {
+            bool good = e[i] >= 0.f && e[i] <= 255.f && rintf(e[i]) == e[i];
+            ok &= good;
+            uint32_t b = good ? (uint32_t)e[i] : 0u;
+            pk |= b << (8 * i);
+            qq += (int)(b * b);
+        }
+        q.u[c] = pk;
     }
-    bool  up   = lane & 4;
-    float send = up ? x[0] : x[1];
-    float keep = up ? x[1] : x[0];
-    float y    = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-    y += __shfl_xor_sync(0xffffffffu, y, 2);
-    y += __shfl_xor_sync(0xffffffffu, y, 1);
-    return y;
-}
-__device__ __forceinline__ uint32_t vidx_of_lane(uint32_t lane) {
-    return ((lane >> 4) & 1u) * 4u + ((lane >> 3) & 1u) * 2u + ((lane >> 2) & 1u);
-}
-__device__ __forceinline__ uint32_t lane_of_vidx(uint32_t j) {
-    return ((j >> 2) & 1u) * 16u + ((j >> 1) & 1u) * 8u + (j & 1u) * 4u;
+    q.qint = __all_sync(0xffffffffu, ok);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) qq += __shfl_xor_sync(0xffffffffu, qq, o);
+    q.qq = qq;
 }
 
-// Squared L2 from the warp's register-resident query chunks to up to 8 rows.
-// ids[j] for j < cnt (uniform across the warp).  Returns, in lane vlane(j),
-// the distance to row j.  All loads are issued before the arithmetic.
-template <typename S, int NCH>
-__device__ __forceinline__ float dist8(const float4 (&q)[NCH], const void* base, const float* scale,
-                                       const uint32_t (&ids)[8], int cnt, uint32_t D,
-                                       uint32_t lane) {
-    const uint32_t nchunk = D >> 2;
-    float4         x[8][NCH];
+// Reduce G per-lane partial sums across the warp with log2(G) exchange levels
+// plus 5 - log2(G) butterfly levels (31 shuffles for G = 32, 9 for G = 8).  On
+// return lane l holds the full sum of value l >> (5 - log2 G).
+template <int G, typename T>
+__device__ __forceinline__ T transpose_reduce(T (&v)[G], uint32_t lane) {
+    constexpr int LOG2G = G == 32 ? 5 : G == 16 ? 4 : G == 8 ? 3 : G == 4 ? 2 : G == 2 ? 1 : 0;
+    static_assert((1 << LOG2G) == G, "G must be a power of two <= 32");
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int lvl = 0; lvl < LOG2G; ++lvl) {
+        const int  half = G >> (lvl + 1);
+        const int  off  = 16 >> lvl;
+        const bool up   = (lane & (uint32_t)off) != 0;
+#pragma unroll
+        for (int i = 0; i < half; ++i) {
+            T send = up ? v[i] : v[i + half];
+            T keep = up ? v[i + half] : v[i];
+            v[i]   = keep + __shfl_xor_sync(0xffffffffu, send, off);
+        }
+    }
+    T y = v[0];
+#pragma unroll
+    for (int off = 16 >> LOG2G; off >= 1; off >>= 1) y += __shfl_xor_sync(0xffffffffu, y, off);
+    return y;
+}
+template <int G>
+__device__ __forceinline__ uint32_t group_slot_of_lane(uint32_t lane) {
+    constexpr int LOG2G = G == 32 ? 5 : G == 16 ? 4 : G == 8 ? 3 : 0;
+    return lane >> (5 - LOG2G);
+}
+template <int G>
+__device__ __forceinline__ bool group_writer(uint32_t lane) {
+    constexpr int LOG2G = G == 32 ? 5 : G == 16 ? 4 : G == 8 ? 3 : 0;
+    return (lane & ((1u << (5 - LOG2G)) - 1u)) == 0u;
+}
+
+// Squared L2 from the query to up to S::kGroup rows ids[0..cnt) (ids in shared
+// memory, cnt uniform across the warp).  Every row's loads are issued before
+// any arithmetic.  Returns, in lane l, the distance to row group_slot_of_lane(l).
+template <typename S, int NCH, typename IdFn>
+__device__ __forceinline__ float dist_group(const Query<NCH>& q, const void* base, const float* scale,
+                                            IdFn ids, int cnt, uint32_t D, uint32_t lane) {
+    constexpr int  G      = S::kGroup;
+    const uint32_t nchunk = D >> 2;
+    typename S::raw_t x[G][NCH];
+    float             sc[G];
+#pragma unroll
+    for (int j = 0; j < G; ++j) {
+        uint32_t id = j < cnt ? ids(j) : 0u;
 #pragma unroll
         for (int c = 0; c < NCH; ++c) {
             uint32_t ch = lane + 32u * c;
-            if (j < cnt && ch < nchunk)
-                x[j][c] = S::load4(base, scale, ids[j], D, ch);
-            else
-                x[j][c] = make_float4(0.f, 0.f, 0.f, 0.f);
+            x[j][c]     = (j < cnt && ch < nchunk) ? S::load(base, id, D, ch) : S::zero();
+        }
+        if constexpr (S::kScaled) sc[j] = j < cnt ? __ldg(scale + id) : 0.f;
+        else sc[j] = 1.f;
+    }
+    if constexpr (S::kBytes8) {
+        if (q.qint) {
+            int v[G];
+#pragma unroll
+            for (int j = 0; j < G; ++j) {
+                int acc = 0;
+#pragma unroll
+                for (int c = 0; c < NCH; ++c) {
+                    int xx = __dp4a((unsigned)x[j][c], (unsigned)x[j][c], 0u);
+                    int qx = __dp4a((unsigned)q.u[c], (unsigned)x[j][c], 0u);
+                    acc += xx - 2 * qx;
+                }
+                v[j] = acc;
+            }
+            int y = transpose_reduce<G, int>(v, lane);
+            return (float)(y + q.qq);
         }
     }
-    float v[8];
+    float v[G];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < G; ++j) {
         float acc = 0.f;
 #pragma unroll
         for (int c = 0; c < NCH; ++c) {
             uint32_t ch = lane + 32u * c;
-            if (j < cnt && ch < nchunk) acc = sqdiff4(q[c], x[j][c], acc);
+            if (ch < nchunk) acc = sqdiff4(q.f[c], S::widen(x[j][c], sc[j]), acc);
         }
         v[j] = acc;
     }
-    return transpose_reduce8(v, lane);
-}
-
-template <int NCH>
-__device__ __forceinline__ void load_query_f32(float4 (&q)[NCH], const float* row, uint32_t D,
-                                               uint32_t lane) {
-    const uint32_t nchunk = D >> 2;
-#pragma unroll
-    for (int c = 0; c < NCH; ++c) {
-        uint32_t ch = lane + 32u * c;
-        q[c] = ch < nchunk ? __ldg(reinterpret_cast<const float4*>(row) + ch)
-                           : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
+    return transpose_reduce<G, float>(v, lane);
 }
 
 // ---------------------------------------------------------------- keys
@@ -198,12 +259,15 @@ __device__ __forceinline__ uint64_t make_key(float d, uint32_t lo) {
 }
 __device__ __forceinline__ float key_dist(uint64_t k) { return __uint_as_float((uint32_t)(k >> 32)); }
 
-// Warp bitonic sort of SPL*32 keys held as key[s] = element s*32 + lane.
+// Warp bitonic sort of the first n (power of two <= SPL*32) keys held as
+// key[s] = element s*32 + lane; elements at or beyond n are not touched.
 template <int SPL>
-__device__ __forceinline__ void warp_bitonic_sort(uint64_t (&key)[SPL], uint32_t lane) {
+__device__ __forceinline__ void warp_bitonic_sort(uint64_t (&key)[SPL], uint32_t lane,
+                                                  uint32_t n = SPL * 32) {
     constexpr int N = SPL * 32;
 #pragma unroll
     for (int k = 2; k <= N; k <<= 1) {
+        if ((uint32_t)k > n) break;
 #pragma unroll
         for (int j = k >> 1; j > 0; j >>= 1) {
             if (j >= 32) {

@@ -20,8 +20,8 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
 // Random R-regular start graph over ids first .. first+n-1 (the reference reads
 // one from a file, utils.cuh:113-148).  Slot j of node i points at
 // first + (i + 1 + h % (n - 1)) % n with h = splitmix64(seed ^ (i * R + j)).
-__global__ void random_graph_kernel(uint32_t* deg, uint32_t* adj, uint64_t first, uint64_t n,
-                                    uint32_t R, uint64_t seed) {
+__global__ void random_graph_kernel(uint32_t* deg, uint32_t* adj, uint32_t* adj_h, uint64_t first,
+                                    uint64_t n, uint32_t R, uint64_t seed) {
     uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (t >= n * R) return;
     uint64_t i = t / R, j = t % R;
@@ -30,16 +30,29 @@ __global__ void random_graph_kernel(uint32_t* deg, uint32_t* adj, uint64_t first
         uint64_t h = splitmix64(seed ^ (i * R + j));
         v          = (uint32_t)(first + (i + 1 + h % (n - 1)) % n);
     }
-    adj[(first + i) * R + j] = v;
+    adj[(first + i) * R + j]   = v;
+    adj_h[(first + i) * R + j] = bloom_pack(v);
     if (j == 0) deg[first + i] = n > 1 ? R : 0u;
 }
 
-cudaError_t launch_random_graph(uint32_t* deg, uint32_t* adj, uint64_t first, uint64_t n,
-                                uint64_t range, uint32_t R, uint64_t seed, cudaStream_t st) {
-    (void)range;
+cudaError_t launch_random_graph(uint32_t* deg, uint32_t* adj, uint32_t* adj_h, uint64_t first,
+                                uint64_t n, uint32_t R, uint64_t seed, cudaStream_t st) {
     uint64_t total = n * R;
     if (total == 0) return cudaSuccess;
-    random_graph_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(deg, adj, first, n, R, seed);
+    random_graph_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(deg, adj, adj_h, first, n, R,
+                                                                        seed);
+    return cudaGetLastError();
+}
+
+__global__ void hash_rows_kernel(const uint32_t* adj, uint32_t* adj_h, uint64_t total) {
+    uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t < total) adj_h[t] = bloom_pack(adj[t]);
+}
+cudaError_t launch_hash_rows(const uint32_t* adj, uint32_t* adj_h, uint64_t n, uint32_t R,
+                             cudaStream_t st) {
+    uint64_t total = n * R;
+    if (total == 0) return cudaSuccess;
+    hash_rows_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(adj, adj_h, total);
     return cudaGetLastError();
 }
 

@@ -115,6 +115,7 @@ struct vann_index {
     float*    fp8_scale = nullptr;
     uint32_t* deg  = nullptr;
     uint32_t* adj  = nullptr;
+    uint32_t* adj_h = nullptr;  // packed filter slots beside every adjacency entry
     uint32_t* tomb = nullptr;
     uint32_t* counters = nullptr;  // ring of work counters
     uint32_t* status   = nullptr;
@@ -136,6 +137,7 @@ struct vann_index {
         cudaFree(fp8_scale);
         cudaFree(deg);
         cudaFree(adj);
+        cudaFree(adj_h);
         cudaFree(tomb);
         cudaFree(counters);
         cudaFree(status);
@@ -192,6 +194,7 @@ struct vann_index {
         a.vecs_f32 = vecs;
         a.deg = deg;
         a.adj = adj;
+        a.adj_h = adj_h;
         a.R = R;
         a.tomb = tomb;
         a.queries = d_q;
@@ -216,6 +219,7 @@ struct vann_index {
         pa.D = p.dim;
         pa.deg = deg;
         pa.adj = adj;
+        pa.adj_h = adj_h;
         pa.R = R;
         pa.alpha = p.alpha;
         pa.cap = MV;
@@ -265,6 +269,7 @@ struct vann_index {
         ra.D = p.dim;
         ra.deg = deg;
         ra.adj = adj;
+        ra.adj_h = adj_h;
         ra.R = R;
         ra.alpha = p.alpha;
         ra.cap = p.max_reverse;
@@ -357,6 +362,7 @@ vann_status vann_create(const vann_params* params, vann_index** out) {
             h->store[0] = h->vecs;
             h->alloc((void**)&h->deg, sizeof(uint32_t) * C);
             h->alloc((void**)&h->adj, sizeof(uint32_t) * C * p.degree);
+            h->alloc((void**)&h->adj_h, sizeof(uint32_t) * C * p.degree);
             h->alloc((void**)&h->tomb, sizeof(uint32_t) * h->tomb_words());
             h->alloc((void**)&h->counters, sizeof(uint32_t) * 32 * kCounterRing);
             h->alloc((void**)&h->status, sizeof(uint32_t) * 32);
@@ -412,6 +418,7 @@ vann_status vann_set_graph(vann_index* h, const float* h_vecs, const uint32_t* h
         VCHECK(cudaMemcpy(h->vecs, h_vecs, sizeof(float) * n * h->p.dim, cudaMemcpyHostToDevice));
         VCHECK(cudaMemcpy(h->deg, h_deg, sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
         VCHECK(cudaMemcpy(h->adj, h_adj, sizeof(uint32_t) * n * R, cudaMemcpyHostToDevice));
+        VCHECK(vann::launch_hash_rows(h->adj, h->adj_h, n, R, 0));
         VCHECK(cudaMemset(h->tomb, 0, sizeof(uint32_t) * h->tomb_words()));
         h->convert_rows(0, n, 0);
         VCHECK(cudaDeviceSynchronize());
@@ -505,7 +512,7 @@ vann_status vann_build(vann_index* h, const float* d_vecs, uint64_t n, uint64_t 
         VCHECK(cudaMemsetAsync(h->deg, 0, sizeof(uint32_t) * n, st));
         h->convert_rows(0, n, st);
         const uint64_t first = (batch == 0 || batch >= n) ? n : batch;
-        VCHECK(vann::launch_random_graph(h->deg, h->adj, 0, first, first, R, seed, st));
+        VCHECK(vann::launch_random_graph(h->deg, h->adj, h->adj_h, 0, first, R, seed, st));
         h->size  = first;
         h->entry = entry != vann::kNone ? entry : h->medoid(first, st);
         VREQUIRE(h->entry < first, VANN_ERR_INVALID, "entry must be inside the first batch");
@@ -543,6 +550,7 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
         a.vecs_f32 = h->vecs;
         a.deg = h->deg;
         a.adj = h->adj;
+        a.adj_h = h->adj_h;
         a.R = h->p.degree;
         a.tomb = h->n_deleted || !h->free_ids.empty() ? h->tomb : nullptr;
         a.queries = d_queries;
@@ -695,6 +703,7 @@ vann_status vann_consolidate(vann_index* h, void* stream) {
         pa.D = h->p.dim;
         pa.deg = h->deg;
         pa.adj = h->adj;
+        pa.adj_h = h->adj_h;
         pa.R = R;
         pa.alpha = h->p.alpha;
         pa.cap = cap;
@@ -734,6 +743,7 @@ vann_status vann_consolidate(vann_index* h, void* stream) {
             a.vecs_f32 = h->vecs;
             a.deg = h->deg;
             a.adj = h->adj;
+        a.adj_h = h->adj_h;
             a.R = R;
             a.tomb = h->tomb;
             a.queries = qv;

@@ -14,6 +14,7 @@ struct SearchArgs {
     const float*    vecs_f32;  // exact rows (rerank)
     const uint32_t* deg;
     const uint32_t* adj;
+    const uint32_t* adj_h;     // packed filter slots of every adjacency entry
     uint32_t        R;
     const uint32_t* tomb;      // tombstone bitmap or null
     const float*    queries;   // nq x D FP32
@@ -46,6 +47,7 @@ struct PruneArgs {
     uint32_t        D;
     uint32_t*       deg;
     uint32_t*       adj;
+    uint32_t*       adj_h;     // packed filter slots, rewritten with adj
     uint32_t        R;
     float           alpha;
     uint32_t        cap;       // merged-list cap (max_visited or max_reverse)
@@ -72,8 +74,10 @@ struct PruneArgs {
 cudaError_t launch_prune(const PruneArgs& a, int num_sms, cudaStream_t st);
 
 // graph utilities (graph_ops.cu)
-cudaError_t launch_random_graph(uint32_t* deg, uint32_t* adj, uint64_t first, uint64_t n,
-                                uint64_t range, uint32_t R, uint64_t seed, cudaStream_t st);
+cudaError_t launch_random_graph(uint32_t* deg, uint32_t* adj, uint32_t* adj_h, uint64_t first,
+                                uint64_t n, uint32_t R, uint64_t seed, cudaStream_t st);
+cudaError_t launch_hash_rows(const uint32_t* adj, uint32_t* adj_h, uint64_t n, uint32_t R,
+                             cudaStream_t st);
 cudaError_t launch_convert(const float* src, void* dst, float* scale, uint64_t rows, uint32_t D,
                            int store, cudaStream_t st);
 cudaError_t launch_iota(uint32_t* out, uint64_t n, uint32_t first, cudaStream_t st);

@@ -32,7 +32,7 @@ struct PruneLayout {
         uint32_t    p = 32;
         while (p < max_cand) p <<= 1;
         l.p2    = p;
-        l.bytes = 8u * p + 4u * p + 4u * p + p + 4u * R;
+        l.bytes = 8u * p + 4u * p + 4u * p + p + 4u * R + 4u * 32u;
         l.bytes = (l.bytes + 15u) & ~15u;
         return l;
     }
@@ -51,6 +51,7 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
     uint8_t*       st   = base + 16u * p2;
     uint32_t*      chosen = reinterpret_cast<uint32_t*>(base + 17u * p2);
     const uint32_t R    = a.R;
+    uint32_t*      plist  = chosen + R;  // positions of one round's candidates
     const bool     rev  = a.csr_off != nullptr;
     const uint32_t chunk = 32u;
 
@@ -75,8 +76,8 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
             const uint32_t w    = w0 + src;
             const uint32_t node = __shfl_sync(0xffffffffu, mynode, src);
 
-            float4 nv[NCH];
-            load_query_f32<NCH>(nv, a.vecs + (uint64_t)node * a.D, a.D, lane);
+            Query<NCH> nv;
+            load_query<NCH>(nv, a.vecs + (uint64_t)node * a.D, a.D, lane);
 
             // --- candidates: A then B
             uint32_t nA = 0, aoff = 0;
@@ -108,14 +109,13 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
             __syncwarp();
             // distances to the node for the reverse sources and B
             const uint32_t dstart = rev ? 0u : nA;
-            uint32_t       ids8[8];
-            for (uint32_t g0 = dstart; g0 < nc; g0 += 8) {
-                int gc = (int)min(8u, nc - g0);
-#pragma unroll
-                for (int j = 0; j < 8; ++j) ids8[j] = j < gc ? cid[g0 + j] : 0u;
-                float    y  = dist8<StoreF32, NCH>(nv, a.vecs, nullptr, ids8, gc, a.D, lane);
-                uint32_t vi = vidx_of_lane(lane);
-                if ((lane & 3u) == 0 && (int)vi < gc) cd[g0 + vi] = y;
+            constexpr int  G      = StoreF32::kGroup;
+            for (uint32_t g0 = dstart; g0 < nc; g0 += G) {
+                int      gc = (int)min((uint32_t)G, nc - g0);
+                float    y  = dist_group<StoreF32, NCH>(nv, a.vecs, nullptr,
+                                                        [&](int j) { return cid[g0 + j]; }, gc, a.D, lane);
+                uint32_t vi = group_slot_of_lane<G>(lane);
+                if (group_writer<G>(lane) && (int)vi < gc) cd[g0 + vi] = y;
             }
             __syncwarp();
             uint32_t ns = 32;
@@ -157,8 +157,8 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
                 __syncwarp();
                 if (ndeg >= R) break;
 
-                float4 pv[NCH];
-                load_query_f32<NCH>(pv, a.vecs + (uint64_t)ps * a.D, a.D, lane);
+                Query<NCH> pv;
+                load_query<NCH>(pv, a.vecs + (uint64_t)ps * a.D, a.D, lane);
                 for (uint32_t c0 = first; c0 < ncap; c0 += 32) {
                     uint32_t i    = c0 + lane;
                     bool     need = false;
@@ -166,25 +166,18 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
                         uint8_t s = st[i];
                         need      = (s & 3u) == kInit && (!a.consistent || ps_a || (s & kFromA));
                     }
-                    uint32_t m = __ballot_sync(0xffffffffu, need);
-                    while (m) {
-                        uint32_t pos8[8];
-                        int      gc = 0;
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            if (m) {
-                                pos8[j] = c0 + __ffs(m) - 1u;
-                                m &= m - 1u;
-                                ++gc;
-                            } else {
-                                pos8[j] = c0;
-                            }
-                            ids8[j] = sid[pos8[j]];
-                        }
-                        float    y  = dist8<StoreF32, NCH>(pv, a.vecs, nullptr, ids8, gc, a.D, lane);
-                        uint32_t vi = vidx_of_lane(lane);
-                        if ((lane & 3u) == 0 && (int)vi < gc) {
-                            uint32_t t = pos8[vi];
+                    uint32_t m  = __ballot_sync(0xffffffffu, need);
+                    uint32_t nm = __popc(m);
+                    if (nm == 0) continue;
+                    if (need) plist[__popc(m & ((1u << lane) - 1u))] = i;
+                    __syncwarp();
+                    for (uint32_t g0 = 0; g0 < nm; g0 += G) {
+                        int      gc = (int)min((uint32_t)G, nm - g0);
+                        float    y  = dist_group<StoreF32, NCH>(
+                            pv, a.vecs, nullptr, [&](int j) { return sid[plist[g0 + j]]; }, gc, a.D, lane);
+                        uint32_t vi = group_slot_of_lane<G>(lane);
+                        if (group_writer<G>(lane) && (int)vi < gc) {
+                            uint32_t t = plist[g0 + vi];
                             if (y * a.alpha <= key_dist(keys[t])) st[t] = (uint8_t)(kPruned | (st[t] & kFromA));
                         }
                     }
@@ -192,7 +185,10 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
                 }
             }
             // rewrite the node's adjacency (in place, like the reference)
-            for (uint32_t t = lane; t < ndeg; t += 32) a.adj[(uint64_t)node * R + t] = chosen[t];
+            for (uint32_t t = lane; t < ndeg; t += 32) {
+                a.adj[(uint64_t)node * R + t]   = chosen[t];
+                a.adj_h[(uint64_t)node * R + t] = bloom_pack(chosen[t]);
+            }
             if (lane == 0) a.deg[node] = ndeg;
             __syncwarp();
         }

@@ -64,6 +64,7 @@ __device__ __forceinline__ uint32_t lower_bound_f(const float* a, uint32_t n, fl
 template <typename S, int NCH, int SPL>
 __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int    G     = S::kGroup;
     const uint32_t   lane  = threadIdx.x & 31u;
     const uint32_t   wib   = threadIdx.x >> 5;
     const SmemLayout lay   = SmemLayout::make(a.L, SPL * 32, a.rerank != 0);
@@ -73,6 +74,7 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
     float*           wl_d  = reinterpret_cast<float*>(base + 5008 + 4 * lay.lp);
     uint32_t*        nb_id = reinterpret_cast<uint32_t*>(base + 5008 + 8 * lay.lp);
     float*           nb_d  = reinterpret_cast<float*>(base + 5008 + 8 * lay.lp + 4 * lay.maxr);
+    uint64_t*        nb_key = reinterpret_cast<uint64_t*>(nb_id);  // same bytes, after the ids/dists are read
     uint64_t*        keys  = reinterpret_cast<uint64_t*>(base + 5008 + 8 * lay.lp + 8 * lay.maxr);
     const uint32_t   L     = a.L;
     const uint32_t   R     = a.R;
@@ -83,8 +85,8 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
         q = __shfl_sync(0xffffffffu, q, 0);
         if (q >= a.nq) break;
 
-        float4 qv[NCH];
-        load_query_f32<NCH>(qv, a.queries + (uint64_t)q * a.D, a.D, lane);
+        Query<NCH> qv;
+        load_query<NCH>(qv, a.queries + (uint64_t)q * a.D, a.D, lane);
         for (uint32_t w = lane; w < kBloomWords; w += 32) bloom[w] = 0u;
 
         uint32_t skip = kNone;
@@ -92,18 +94,15 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
         if (a.skip_mode == 2) skip = a.skip_base + q;
 
         // initializeWorklist: entry visited, distance computed, not in the filter
-        uint32_t ids8[8];
-        ids8[0] = a.entry;
-#pragma unroll
-        for (int j = 1; j < 8; ++j) ids8[j] = 0;
-        float d0 = dist8<S, NCH>(qv, a.store, a.scale, ids8, 1, a.D, lane);
+        const uint32_t entry = a.entry;
+        float d0 = dist_group<S, NCH>(qv, a.store, a.scale, [&](int) { return entry; }, 1, a.D, lane);
         d0       = __shfl_sync(0xffffffffu, d0, 0);
         if (lane == 0) {
-            wl_id[0] = a.entry | kVisitedBit;
+            wl_id[0] = entry | kVisitedBit;
             wl_d[0]  = d0;
         }
         __syncwarp();
-        uint32_t n = 1, parent = a.entry, ppos = 0, hops = 0, nv = 0, evals = 1, adjw = 0;
+        uint32_t n = 1, parent = entry, ppos = 0, hops = 0, nv = 0, evals = 1, adjw = 0;
         float    pd = d0;
 
         for (;;) {
@@ -119,24 +118,33 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
                 }
                 ++nv;
             }
+            // degree and adjacency row in one round trip
+            const uint32_t* row  = a.adj + (uint64_t)parent * R;
+            const uint32_t* rowh = a.adj_h + (uint64_t)parent * R;
+            uint32_t        nid[SPL], hp[SPL];
+#pragma unroll
+            for (int s = 0; s < SPL; ++s) {
+                uint32_t j = (uint32_t)s * 32u + lane;
+                nid[s]     = j < R ? __ldg(row + j) : 0u;
+                hp[s]      = j < R ? __ldg(rowh + j) : 0u;
+            }
             uint32_t dg = __ldg(a.deg + parent);
             dg          = dg < R ? dg : R;
             adjw += dg;
-            const uint32_t* row = a.adj + (uint64_t)parent * R;
 
-            // filterNeighbors: snapshot check of every slot, then mark
-            uint32_t nid[SPL], h1[SPL], h2[SPL];
+            // filterNeighbors: every slot checks the filter as it stood before this
+            // expansion, then the new neighbours are marked
+            uint32_t h1[SPL], h2[SPL];
             bool     pass[SPL];
 #pragma unroll
             for (int s = 0; s < SPL; ++s) {
                 uint32_t j  = (uint32_t)s * 32u + lane;
                 bool     ok = j < dg;
-                nid[s]      = ok ? __ldg(row + j) : 0u;
                 if (ok && a.tomb != nullptr) ok = !((__ldg(a.tomb + (nid[s] >> 5)) >> (nid[s] & 31u)) & 1u);
                 if (ok && nid[s] == skip) ok = false;
+                h1[s] = hp[s] >> 16;
+                h2[s] = hp[s] & 0xffffu;
                 if (ok) {
-                    h1[s] = bloom_h1(nid[s]);
-                    h2[s] = bloom_h2(nid[s]);
                     bool seen = ((bloom[h1[s] >> 5] >> (h1[s] & 31u)) & 1u) &&
                                 ((bloom[h2[s] >> 5] >> (h2[s] & 31u)) & 1u);
                     ok = !seen;
@@ -158,37 +166,65 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
             __syncwarp();
             evals += cnt;
 
-            // distances of the new neighbours, 8 rows per round
-            for (uint32_t g0 = 0; g0 < cnt; g0 += 8) {
-                int gc = (int)min(8u, cnt - g0);
-#pragma unroll
-                for (int j = 0; j < 8; ++j) ids8[j] = j < gc ? nb_id[g0 + j] : 0u;
-                float    y  = dist8<S, NCH>(qv, a.store, a.scale, ids8, gc, a.D, lane);
-                uint32_t vi = vidx_of_lane(lane);
-                if ((lane & 3u) == 0 && (int)vi < gc) nb_d[g0 + vi] = y;
+            // distances: G rows per gather round, all loads of a round in flight
+            for (uint32_t g0 = 0; g0 < cnt; g0 += G) {
+                int   gc = (int)min((uint32_t)G, cnt - g0);
+                float y  = dist_group<S, NCH>(qv, a.store, a.scale,
+                                              [&](int j) { return nb_id[g0 + j]; }, gc, a.D, lane);
+                uint32_t vi = group_slot_of_lane<G>(lane);
+                if (group_writer<G>(lane) && (int)vi < gc) nb_d[g0 + vi] = y;
             }
             __syncwarp();
 
-            if (cnt > 0) {
-                // sort the new neighbours by (distance, id)
-                uint64_t key[SPL];
+            // candidates that cannot enter a full worklist are dropped before the
+            // sort: with n == L a new entry with d >= wl_d[L-1] lands at >= L
+            const float tail = n == L ? wl_d[L - 1] : __int_as_float(0x7f800000);
+            uint64_t    key[SPL];
+            bool        keep[SPL];
+#pragma unroll
+            for (int s = 0; s < SPL; ++s) {
+                uint32_t j = (uint32_t)s * 32u + lane;
+                keep[s]    = false;
+                key[s]     = ~0ull;
+                if (j < cnt) {
+                    float dd = nb_d[j];
+                    keep[s]  = n < L || dd < tail;
+                    key[s]   = make_key(dd, nb_id[j]);
+                }
+            }
+            __syncwarp();
+            uint32_t kc = 0;
+#pragma unroll
+            for (int s = 0; s < SPL; ++s) {
+                uint32_t m = __ballot_sync(0xffffffffu, keep[s]);
+                if (keep[s]) nb_key[kc + __popc(m & ((1u << lane) - 1u))] = key[s];
+                kc += __popc(m);
+            }
+            __syncwarp();
+
+            if (kc > 0) {
+                // sort the kept candidates by (distance, id) with the smallest network
+                uint32_t n2 = 1;
+                while (n2 < kc) n2 <<= 1;
 #pragma unroll
                 for (int s = 0; s < SPL; ++s) {
                     uint32_t j = (uint32_t)s * 32u + lane;
-                    key[s]     = j < cnt ? make_key(nb_d[j], nb_id[j]) : ~0ull;
+                    key[s]     = j < kc ? nb_key[j] : ~0ull;
                 }
-                if (cnt <= 32) {
-                    uint64_t k1[1] = {key[0]};
-                    warp_bitonic_sort<1>(k1, lane);
-                    key[0] = k1[0];
-                } else {
-                    warp_bitonic_sort<SPL>(key, lane);
+                if (n2 > 1) {
+                    if (n2 <= 32) {
+                        uint64_t k1[1] = {key[0]};
+                        warp_bitonic_sort<1>(k1, lane, n2);
+                        key[0] = k1[0];
+                    } else {
+                        warp_bitonic_sort<SPL>(key, lane, n2);
+                    }
                 }
                 __syncwarp();
 #pragma unroll
                 for (int s = 0; s < SPL; ++s) {
                     uint32_t j = (uint32_t)s * 32u + lane;
-                    if (j < cnt) {
+                    if (j < kc) {
                         nb_id[j] = (uint32_t)key[s];
                         nb_d[j]  = key_dist(key[s]);
                     }
@@ -201,7 +237,7 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
 #pragma unroll
                 for (int s = 0; s < SPL; ++s) {
                     uint32_t j = (uint32_t)s * 32u + lane;
-                    pj[s]      = j < cnt ? j + upper_bound_f(wl_d, n, nb_d[j]) : L;
+                    pj[s]      = j < kc ? j + upper_bound_f(wl_d, n, nb_d[j]) : L;
                 }
                 uint32_t p0 = __shfl_sync(0xffffffffu, pj[0], 0);
                 if (p0 < L) {
@@ -214,7 +250,7 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
                             if (i < n) {
                                 id = wl_id[i];
                                 dd = wl_d[i];
-                                np = i + lower_bound_f(nb_d, cnt, dd);
+                                np = i + lower_bound_f(nb_d, kc, dd);
                             }
                             __syncwarp();
                             if (np < L) {
@@ -227,15 +263,15 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
 #pragma unroll
                     for (int s = 0; s < SPL; ++s) {
                         uint32_t j = (uint32_t)s * 32u + lane;
-                        if (j < cnt && pj[s] < L) {
+                        if (j < kc && pj[s] < L) {
                             wl_id[pj[s]] = nb_id[j];
                             wl_d[pj[s]]  = nb_d[j];
                         }
                     }
-                    n = min(n + cnt, L);
+                    n = min(n + kc, L);
+                    if (p0 < ppos + 1u) ppos = p0 - 1u;  // rescan from p0
                 }
                 __syncwarp();
-                if (p0 < ppos + 1u) ppos = p0 - 1u;  // rescan from p0
             }
 
             // next parent: first unvisited entry
@@ -263,13 +299,14 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
         if (a.out_ids != nullptr) {
             if (a.rerank) {
                 // exact FP32 distances of the final worklist, sorted (dist, position)
-                for (uint32_t g0 = 0; g0 < n; g0 += 8) {
-                    int gc = (int)min(8u, n - g0);
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) ids8[j] = j < gc ? (wl_id[g0 + j] & ~kVisitedBit) : 0u;
-                    float    y  = dist8<StoreF32, NCH>(qv, a.vecs_f32, nullptr, ids8, gc, a.D, lane);
-                    uint32_t vi = vidx_of_lane(lane);
-                    if ((lane & 3u) == 0 && (int)vi < gc) keys[g0 + vi] = make_key(y, g0 + vi);
+                constexpr int GF = StoreF32::kGroup;
+                for (uint32_t g0 = 0; g0 < n; g0 += GF) {
+                    int   gc = (int)min((uint32_t)GF, n - g0);
+                    float y  = dist_group<StoreF32, NCH>(
+                        qv, a.vecs_f32, nullptr, [&](int j) { return wl_id[g0 + j] & ~kVisitedBit; }, gc, a.D,
+                        lane);
+                    uint32_t vi = group_slot_of_lane<GF>(lane);
+                    if (group_writer<GF>(lane) && (int)vi < gc) keys[g0 + vi] = make_key(y, g0 + vi);
                 }
                 __syncwarp();
                 for (uint32_t i = n + lane; i < lay.keys; i += 32) keys[i] = ~0ull;

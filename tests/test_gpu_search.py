@@ -57,14 +57,21 @@ def test_search_r32_and_padding(oracle, vann_mod, graph32):
     st, oids, od, _, _ = g.search(q, 75, 75, entry, skip_mode=1)
     assert np.array_equal(ids.cpu().numpy().view(np.uint32), oids)
     assert np.array_equal(d.cpu().numpy(), od)
-    # a 2-node graph pads the tail with UINT32_MAX / +inf
+    # a 2-node graph pads the tail with UINT32_MAX / +inf.  The entry sits in the
+    # worklist but never in the bloom filter (search.cuh:30-58), so it is found
+    # again as node 1's neighbour: 3 entries, the entry twice.
     tiny = vann_mod.Index(128, 32, 8, 1.2, capacity=4)
     adj = np.zeros((2, 32), np.uint32)
     adj[0, 0], adj[1, 0] = 1, 0
     tiny.set_graph(base[:2], np.array([1, 1], np.uint32), adj, 0)
     ids, d = tiny.search(torch.from_numpy(q[:3]).cuda(), k=5, L=8)
     ids = ids.cpu().numpy().view(np.uint32)
-    assert (ids[:, 2:] == 0xFFFFFFFF).all() and np.isinf(d.cpu().numpy()[:, 2:]).all()
+    assert (ids[:, 3:] == 0xFFFFFFFF).all() and np.isinf(d.cpu().numpy()[:, 3:]).all()
+    for row in ids[:, :3]:
+        assert sorted(row.tolist()) == [0, 0, 1]
+    tg = oracle.Graph(base[:2], np.array([1, 1], np.uint32), adj)
+    st, oids, _, _, _ = tg.search(q[:3], 8, 5, 0)
+    assert np.array_equal(ids, oids)
 
 
 def test_bf16_store_is_exact_on_integer_data(oracle, vann_mod, graph64):
