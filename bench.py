@@ -192,6 +192,17 @@ def main():
             sweep.setdefault(name, []).append((L, recall(torch, ids, gt)))
     idx.sync()
 
+    # autotune the search variant of every form at its operating point
+    def op_point0(name):
+        for L, r in sweep[name]:
+            if r >= TARGET:
+                return L
+        return sweep[name][-1][0]
+
+    for store, rr in forms:
+        name = store + ("+rerank" if rr else "")
+        idx.autotune(q_d, k=K, L=op_point0(name), store=store, rerank=rr)
+
     def op_point(name):
         for L, r in sweep[name]:
             if r >= TARGET:

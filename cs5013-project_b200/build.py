@@ -20,8 +20,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-ccbin", "g++",
          "--expt-relaxed-constexpr", "-Wno-deprecated-gpu-targets"]
-SOURCES = ["search.cu", "prune.cu", "graph_ops.cu", "index.cu"]
-HEADERS = ["common.cuh", "kernels.h"]
+SOURCES = ["search.cu", "search_f32.cu", "search_bf16.cu", "search_fp8.cu", "search_u8.cu", "prune.cu",
+           "graph_ops.cu", "index.cu"]
+HEADERS = ["common.cuh", "kernels.h", "search_impl.cuh"]
 
 
 def _stale(obj: str, src: str) -> bool:

@@ -55,201 +55,236 @@ __device__ __forceinline__ uint32_t bloom_h2(uint32_t x) {
 __device__ __forceinline__ uint32_t bloom_pack(uint32_t x) { return (bloom_h1(x) << 16) | bloom_h2(x); }
 
 // ---------------------------------------------------------------- stores
-// Each store reads one 4-element chunk of a row per lane (16, 8 or 4 bytes), so
-// a warp reads a whole 128-dim row in one coalesced request.  kGroup rows are
-// gathered per round (32 registers of raw data per lane whatever the width):
-// narrower elements mean fewer dependent gather rounds per expansion.
+// Rows are read in 16-byte chunks: 4 FP32, 8 BF16 or 16 one-byte elements.  A
+// row of C chunks is spread over T = C lanes (T <= 32, CPL chunks per lane when
+// C > 32), so one warp load instruction reads 32 / T whole rows, coalesced, and
+// each lane reduces 16 bytes before a log2(T)-level shuffle reduction.  M rows
+// per lane group are gathered per round with all loads in flight first, so a
+// round covers G = M * 32 / T rows: 8 (FP32), 16 (BF16) or 32 (one-byte rows).
+// Dimension class DC: D <= 128 << DC.
 struct StoreF32 {
-    static constexpr int  kGroup  = 8;
-    static constexpr bool kScaled = false;
-    static constexpr bool kBytes8 = false;
-    using raw_t                   = float4;
-    __device__ __forceinline__ static raw_t load(const void* base, uint64_t row, uint32_t D, uint32_t c) {
-        return __ldg(reinterpret_cast<const float4*>(static_cast<const float*>(base) + row * D) + c);
+    static constexpr int  kElems = 4, kLanes128 = 32, kM = 8;
+    static constexpr bool kScaled = false, kInt = false;
+    __device__ __forceinline__ static void widen(const uint4& r, float, float (&o)[4]) {
+        o[0] = __uint_as_float(r.x);
+        o[1] = __uint_as_float(r.y);
+        o[2] = __uint_as_float(r.z);
+        o[3] = __uint_as_float(r.w);
     }
-    __device__ __forceinline__ static raw_t zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
-    __device__ __forceinline__ static float4 widen(const raw_t& x, float) { return x; }
 };
 struct StoreBF16 {
-    static constexpr int  kGroup  = 16;
-    static constexpr bool kScaled = false;
-    static constexpr bool kBytes8 = false;
-    using raw_t                   = uint2;
-    __device__ __forceinline__ static raw_t load(const void* base, uint64_t row, uint32_t D, uint32_t c) {
-        return __ldg(reinterpret_cast<const uint2*>(static_cast<const __nv_bfloat16*>(base) + row * D) + c);
-    }
-    __device__ __forceinline__ static raw_t zero() { return make_uint2(0u, 0u); }
-    __device__ __forceinline__ static float4 widen(const raw_t& u, float) {
-        return make_float4(__uint_as_float(u.x << 16), __uint_as_float(u.x & 0xffff0000u),
-                           __uint_as_float(u.y << 16), __uint_as_float(u.y & 0xffff0000u));
+    static constexpr int  kElems = 8, kLanes128 = 16, kM = 8;
+    static constexpr bool kScaled = false, kInt = false;
+    __device__ __forceinline__ static void widen(const uint4& r, float, float (&o)[8]) {
+        const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            o[2 * i]     = __uint_as_float(w[i] << 16);
+            o[2 * i + 1] = __uint_as_float(w[i] & 0xffff0000u);
+        }
     }
 };
 struct StoreFP8 {
-    static constexpr int  kGroup  = 16;
-    static constexpr bool kScaled = true;
-    static constexpr bool kBytes8 = false;
-    using raw_t                   = uint32_t;
-    __device__ __forceinline__ static raw_t load(const void* base, uint64_t row, uint32_t D, uint32_t c) {
-        return __ldg(reinterpret_cast<const uint32_t*>(static_cast<const uint8_t*>(base) + row * D) + c);
-    }
-    __device__ __forceinline__ static raw_t zero() { return 0u; }
-    __device__ __forceinline__ static float4 widen(const raw_t& u, float s) {
-        __half2_raw lo = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(u & 0xffffu), __NV_E4M3);
-        __half2_raw hi = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(u >> 16), __NV_E4M3);
-        float2 a = __half22float2(*reinterpret_cast<__half2*>(&lo));
-        float2 b = __half22float2(*reinterpret_cast<__half2*>(&hi));
-        return make_float4(a.x * s, a.y * s, b.x * s, b.y * s);
+    static constexpr int  kElems = 16, kLanes128 = 8, kM = 8;
+    static constexpr bool kScaled = true, kInt = false;
+    __device__ __forceinline__ static void widen(const uint4& r, float s, float (&o)[16]) {
+        const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            __half2_raw lo = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[i] & 0xffffu), __NV_E4M3);
+            __half2_raw hi = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[i] >> 16), __NV_E4M3);
+            float2 a = __half22float2(*reinterpret_cast<__half2*>(&lo));
+            float2 b = __half22float2(*reinterpret_cast<__half2*>(&hi));
+            o[4 * i]     = a.x * s;
+            o[4 * i + 1] = a.y * s;
+            o[4 * i + 2] = b.x * s;
+            o[4 * i + 3] = b.y * s;
+        }
     }
 };
 struct StoreU8 {
-    static constexpr int  kGroup  = 32;
-    static constexpr bool kScaled = false;
-    static constexpr bool kBytes8 = true;  // exact integer path for integer queries
-    using raw_t                   = uint32_t;
-    __device__ __forceinline__ static raw_t load(const void* base, uint64_t row, uint32_t D, uint32_t c) {
-        return __ldg(reinterpret_cast<const uint32_t*>(static_cast<const uint8_t*>(base) + row * D) + c);
-    }
-    __device__ __forceinline__ static raw_t zero() { return 0u; }
-    __device__ __forceinline__ static float4 widen(const raw_t& u, float) {
-        return make_float4((float)(u & 0xffu), (float)((u >> 8) & 0xffu), (float)((u >> 16) & 0xffu),
-                           (float)(u >> 24));
+    static constexpr int  kElems = 16, kLanes128 = 8, kM = 8;
+    static constexpr bool kScaled = false, kInt = true;  // exact dp4a path for integer queries
+    __device__ __forceinline__ static void widen(const uint4& r, float, float (&o)[16]) {
+        const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            o[4 * i]     = (float)(w[i] & 0xffu);
+            o[4 * i + 1] = (float)((w[i] >> 8) & 0xffu);
+            o[4 * i + 2] = (float)((w[i] >> 16) & 0xffu);
+            o[4 * i + 3] = (float)(w[i] >> 24);
+        }
     }
 };
 
-__device__ __forceinline__ float sqdiff4(const float4& q, const float4& x, float acc) {
-    float d0 = q.x - x.x, d1 = q.y - x.y, d2 = q.z - x.z, d3 = q.w - x.w;
-    acc      = fmaf(d0, d0, acc);
-    acc      = fmaf(d1, d1, acc);
-    acc      = fmaf(d2, d2, acc);
-    acc      = fmaf(d3, d3, acc);
-    return acc;
+// lanes per row and chunks per lane of store S in dimension class DC
+template <typename S, int DC>
+struct Layout {
+    static constexpr int kChunks128 = S::kLanes128;
+    static constexpr int kT   = (S::kLanes128 << DC) < 32 ? (S::kLanes128 << DC) : 32;
+    static constexpr int kCPL = (S::kLanes128 << DC) / kT;
+    static constexpr int kP   = 32 / kT;          // rows per warp load
+    static constexpr int kG   = S::kM * kP;       // rows per gather round
+};
+
+__device__ __forceinline__ uint4 load16(const void* base, uint64_t row_bytes, uint64_t row, uint32_t k) {
+    return __ldg(reinterpret_cast<const uint4*>(static_cast<const unsigned char*>(base) + row * row_bytes) + k);
 }
 
-// Register-resident query: FP32 chunks, plus packed uint8 chunks and |q|^2 when
-// every element is an integer in [0, 255] (then uint8 rows use dp4a exactly).
-template <int NCH>
+// Register-resident query in the lane layout of store S: the lane's chunks in
+// FP32, plus packed uint8 words and |q|^2 when every element is an integer in
+// [0, 255] (uint8 rows then use exact dp4a integer arithmetic).
+template <typename S, int DC>
 struct Query {
-    float4   f[NCH];
-    uint32_t u[NCH];
+    float    f[Layout<S, DC>::kCPL][S::kElems];
+    uint32_t u[Layout<S, DC>::kCPL][S::kElems / 4];
     int      qq;
     bool     qint;
 };
 
-template <int NCH>
-__device__ __forceinline__ void load_query(Query<NCH>& q, const float* row, uint32_t D, uint32_t lane) {
-    const uint32_t nchunk = D >> 2;
+template <typename S, int DC>
+__device__ __forceinline__ void load_query(Query<S, DC>& q, const float* row, uint32_t D, uint32_t lane) {
+    using Ly              = Layout<S, DC>;
+    const uint32_t chunks = D / S::kElems;
+    const uint32_t t      = lane % Ly::kT;
     bool           ok     = true;
     int            qq     = 0;
 #pragma unroll
-    for (int c = 0; c < NCH; ++c) {
-        uint32_t ch = lane + 32u * c;
-        float4   v  = ch < nchunk ? __ldg(reinterpret_cast<const float4*>(row) + ch)
-                                  : make_float4(0.f, 0.f, 0.f, 0.f);
-        q.f[c]      = v;
-        float e[4]  = {v.x, v.y, v.z, v.w};
-        uint32_t pk = 0;
+    for (int c = 0; c < Ly::kCPL; ++c) {
+        uint32_t k     = t + (uint32_t)Ly::kT * c;
+        bool     valid = k < chunks;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            bool good = e[i] >= 0.f && e[i] <= 255.f && rintf(e[i]) == e[i];
-            ok &= good;
-            uint32_t b = good ? (uint32_t)e[i] : 0u;
-            pk |= b << (8 * i);
-            qq += (int)(b * b);
+        for (int v = 0; v < S::kElems / 4; ++v) {
+            float4 x = valid ? __ldg(reinterpret_cast<const float4*>(row + k * S::kElems) + v)
+                             : make_float4(0.f, 0.f, 0.f, 0.f);
+            float  e[4] = {x.x, x.y, x.z, x.w};
+            uint32_t pk = 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                q.f[c][4 * v + i] = e[i];
+                bool good         = e[i] >= 0.f && e[i] <= 255.f && rintf(e[i]) == e[i];
+                ok &= good;
+                uint32_t b = good ? (uint32_t)e[i] : 0u;
+                pk |= b << (8 * i);
+                qq += (int)(b * b);
+            }
+            q.u[c][v] = pk;
         }
-        q.u[c] = pk;
     }
     q.qint = __all_sync(0xffffffffu, ok);
+    // each group of T lanes holds the whole query
 #pragma unroll
-    for (int o = 16; o; o >>= 1) qq += __shfl_xor_sync(0xffffffffu, qq, o);
+    for (int o = Ly::kT / 2; o >= 1; o >>= 1) qq += __shfl_xor_sync(0xffffffffu, qq, o);
     q.qq = qq;
 }
 
-// Reduce G per-lane partial sums across the warp with log2(G) exchange levels
-// plus 5 - log2(G) butterfly levels (31 shuffles for G = 32, 9 for G = 8).  On
-// return lane l holds the full sum of value l >> (5 - log2 G).
-template <int G, typename T>
-__device__ __forceinline__ T transpose_reduce(T (&v)[G], uint32_t lane) {
-    constexpr int LOG2G = G == 32 ? 5 : G == 16 ? 4 : G == 8 ? 3 : G == 4 ? 2 : G == 2 ? 1 : 0;
-    static_assert((1 << LOG2G) == G, "G must be a power of two <= 32");
+__device__ __forceinline__ float sqdiff(float q, float x, float acc) {
+    float d = q - x;
+    return fmaf(d, d, acc);
+}
+
+// Reduce M per-lane values across the T lanes of each lane group: log2(M)
+// exchange levels then butterfly levels.  Lane t of a group ends with the sum
+// of value t / (T / M).
+template <int M, int T, typename V>
+__device__ __forceinline__ V group_reduce(V (&v)[M], uint32_t lane) {
+    constexpr int LOG2M = M == 32 ? 5 : M == 16 ? 4 : M == 8 ? 3 : M == 4 ? 2 : M == 2 ? 1 : 0;
+    static_assert((1 << LOG2M) == M && M <= T, "M must be a power of two <= T");
 #pragma unroll
-    for (int lvl = 0; lvl < LOG2G; ++lvl) {
-        const int  half = G >> (lvl + 1);
-        const int  off  = 16 >> lvl;
+    for (int lvl = 0; lvl < LOG2M; ++lvl) {
+        const int  half = M >> (lvl + 1);
+        const int  off  = (T / 2) >> lvl;
         const bool up   = (lane & (uint32_t)off) != 0;
 #pragma unroll
         for (int i = 0; i < half; ++i) {
-            T send = up ? v[i] : v[i + half];
-            T keep = up ? v[i + half] : v[i];
+            V send = up ? v[i] : v[i + half];
+            V keep = up ? v[i + half] : v[i];
             v[i]   = keep + __shfl_xor_sync(0xffffffffu, send, off);
         }
     }
-    T y = v[0];
+    V y = v[0];
 #pragma unroll
-    for (int off = 16 >> LOG2G; off >= 1; off >>= 1) y += __shfl_xor_sync(0xffffffffu, y, off);
+    for (int off = (T / 2) >> LOG2M; off >= 1; off >>= 1) y += __shfl_xor_sync(0xffffffffu, y, off);
     return y;
 }
-template <int G>
-__device__ __forceinline__ uint32_t group_slot_of_lane(uint32_t lane) {
-    constexpr int LOG2G = G == 32 ? 5 : G == 16 ? 4 : G == 8 ? 3 : 0;
-    return lane >> (5 - LOG2G);
+
+// Row (within a gather round) whose distance lane `lane` holds after dist_group,
+// and whether this lane is the one that writes it.
+template <typename S, int DC>
+__device__ __forceinline__ uint32_t round_row_of_lane(uint32_t lane) {
+    using Ly        = Layout<S, DC>;
+    const uint32_t t = lane % Ly::kT, g = lane / Ly::kT;
+    return (t / (Ly::kT / S::kM)) * Ly::kP + g;
 }
-template <int G>
-__device__ __forceinline__ bool group_writer(uint32_t lane) {
-    constexpr int LOG2G = G == 32 ? 5 : G == 16 ? 4 : G == 8 ? 3 : 0;
-    return (lane & ((1u << (5 - LOG2G)) - 1u)) == 0u;
+template <typename S, int DC>
+__device__ __forceinline__ bool round_writer(uint32_t lane) {
+    using Ly = Layout<S, DC>;
+    return (lane % (Ly::kT / S::kM)) == 0u;
 }
 
-// Squared L2 from the query to up to S::kGroup rows ids[0..cnt) (ids in shared
-// memory, cnt uniform across the warp).  Every row's loads are issued before
-// any arithmetic.  Returns, in lane l, the distance to row group_slot_of_lane(l).
-template <typename S, int NCH, typename IdFn>
-__device__ __forceinline__ float dist_group(const Query<NCH>& q, const void* base, const float* scale,
+// Squared L2 from the query to rows ids(0) .. ids(cnt-1), cnt <= kG (uniform
+// across the warp).  All loads are issued before any arithmetic.  The result
+// for row round_row_of_lane(lane) is returned in the lanes where round_writer.
+template <typename S, int DC, typename IdFn>
+__device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* base, const float* scale,
                                             IdFn ids, int cnt, uint32_t D, uint32_t lane) {
-    constexpr int  G      = S::kGroup;
-    const uint32_t nchunk = D >> 2;
-    typename S::raw_t x[G][NCH];
-    float             sc[G];
+    using Ly                 = Layout<S, DC>;
+    constexpr int  M         = S::kM;
+    const uint32_t chunks    = D / S::kElems;
+    const uint64_t row_bytes = (uint64_t)D * (16 / S::kElems);
+    const uint32_t t         = lane % Ly::kT;
+    const uint32_t g         = lane / Ly::kT;
+    uint4          x[M][Ly::kCPL];
+    float          sc[M];
 #pragma unroll
-    for (int j = 0; j < G; ++j) {
-        uint32_t id = j < cnt ? ids(j) : 0u;
+    for (int m = 0; m < M; ++m) {
+        const int r     = m * Ly::kP + (int)g;
+        const bool valid = r < cnt;
+        uint32_t   id    = valid ? ids(r) : 0u;
 #pragma unroll
-        for (int c = 0; c < NCH; ++c) {
-            uint32_t ch = lane + 32u * c;
-            x[j][c]     = (j < cnt && ch < nchunk) ? S::load(base, id, D, ch) : S::zero();
+        for (int c = 0; c < Ly::kCPL; ++c) {
+            uint32_t k = t + (uint32_t)Ly::kT * c;
+            x[m][c]    = (valid && k < chunks) ? load16(base, row_bytes, id, k) : make_uint4(0u, 0u, 0u, 0u);
         }
-        if constexpr (S::kScaled) sc[j] = j < cnt ? __ldg(scale + id) : 0.f;
-        else sc[j] = 1.f;
+        if constexpr (S::kScaled) sc[m] = valid ? __ldg(scale + id) : 0.f;
+        else sc[m] = 1.f;
     }
-    if constexpr (S::kBytes8) {
+    if constexpr (S::kInt) {
         if (q.qint) {
-            int v[G];
+            int v[M];
 #pragma unroll
-            for (int j = 0; j < G; ++j) {
-                int acc = 0;
+            for (int m = 0; m < M; ++m) {
+                unsigned xx = 0u, qx = 0u;
 #pragma unroll
-                for (int c = 0; c < NCH; ++c) {
-                    int xx = __dp4a((unsigned)x[j][c], (unsigned)x[j][c], 0u);
-                    int qx = __dp4a((unsigned)q.u[c], (unsigned)x[j][c], 0u);
-                    acc += xx - 2 * qx;
+                for (int c = 0; c < Ly::kCPL; ++c) {
+                    const unsigned w[4] = {x[m][c].x, x[m][c].y, x[m][c].z, x[m][c].w};
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        xx = __dp4a(w[i], w[i], xx);
+                        qx = __dp4a((unsigned)q.u[c][i], w[i], qx);
+                    }
                 }
-                v[j] = acc;
+                v[m] = (int)xx - 2 * (int)qx;
             }
-            int y = transpose_reduce<G, int>(v, lane);
+            int y = group_reduce<M, Ly::kT, int>(v, lane);
             return (float)(y + q.qq);
         }
     }
-    float v[G];
+    float v[M];
 #pragma unroll
-    for (int j = 0; j < G; ++j) {
-        float acc = 0.f;
+    for (int m = 0; m < M; ++m) v[m] = 0.f;
 #pragma unroll
-        for (int c = 0; c < NCH; ++c) {
-            uint32_t ch = lane + 32u * c;
-            if (ch < nchunk) acc = sqdiff4(q.f[c], S::widen(x[j][c], sc[j]), acc);
+    for (int c = 0; c < Ly::kCPL; ++c) {
+        float e[M][S::kElems];
+#pragma unroll
+        for (int m = 0; m < M; ++m) S::widen(x[m][c], sc[m], e[m]);
+#pragma unroll
+        for (int i = 0; i < S::kElems; ++i) {
+#pragma unroll
+            for (int m = 0; m < M; ++m) v[m] = sqdiff(q.f[c][i], e[m][i], v[m]);
         }
-        v[j] = acc;
     }
-    return transpose_reduce<G, float>(v, lane);
+    return group_reduce<M, Ly::kT, float>(v, lane);
 }
 
 // ---------------------------------------------------------------- keys

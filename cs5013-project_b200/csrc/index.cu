@@ -12,6 +12,8 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <map>
+#include <tuple>
 #include <new>
 #include <string>
 #include <vector>
@@ -123,6 +125,13 @@ struct vann_index {
     size_t    held     = 0;
 
     std::vector<uint32_t> free_ids;  // consolidated ids, reused by inserts
+    // autotuned search variant per (store, rerank, L)
+    std::map<std::tuple<uint32_t, uint32_t, uint32_t>, int> tuned;
+
+    int variant_for(const vann_search_params& sp) const {
+        auto it = tuned.find(std::make_tuple(sp.store, sp.rerank ? 1u : 0u, sp.L));
+        return it == tuned.end() ? 0 : it->second;
+    }
 
     DevBuf vis_ids, vis_d, vis_n, nodes, e_keys, e_vals, e_keys2, e_vals2, counts, offsets, cub_tmp,
         medoid_ws, gather, cand, cand_n, cand_d, list_n, out_tmp;
@@ -569,7 +578,45 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
         a.adjw_out = d_adjw;
         a.counter = h->next_counter(S(stream));
         a.status = h->status;
-        VCHECK(vann::launch_search(a, (int)sp->store, h->num_sms, S(stream)));
+        VCHECK(vann::launch_search(a, (int)sp->store, h->num_sms, S(stream), h->variant_for(*sp)));
+    });
+}
+
+vann_status vann_autotune(vann_index* h, const float* d_queries, uint64_t nq, const vann_search_params* sp,
+                          void* stream) {
+    return guard([&] {
+        VREQUIRE(h && sp && d_queries && nq > 0, VANN_ERR_INVALID, "null argument");
+        cudaStream_t st = S(stream);
+        h->out_tmp.ensure((sizeof(uint32_t) + sizeof(float)) * nq * sp->k);
+        uint32_t*   ids = h->out_tmp.as<uint32_t>();
+        float*      dd  = reinterpret_cast<float*>(ids + nq * sp->k);
+        cudaEvent_t e0, e1;
+        VCHECK(cudaEventCreate(&e0));
+        VCHECK(cudaEventCreate(&e1));
+        const auto key = std::make_tuple(sp->store, sp->rerank ? 1u : 0u, sp->L);
+        int   best = 0;
+        float best_ms = 1e30f;
+        for (int v = 0; v < vann::search_variants(); ++v) {
+            h->tuned[key] = v;
+            float ms_sum = 0.f;
+            for (int rep = 0; rep < 4; ++rep) {
+                VCHECK(cudaEventRecord(e0, st));
+                vann_status s2 = vann_search(h, d_queries, nq, sp, ids, dd, stream);
+                VREQUIRE(s2 == VANN_OK, s2, g_last_error);
+                VCHECK(cudaEventRecord(e1, st));
+                VCHECK(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                VCHECK(cudaEventElapsedTime(&ms, e0, e1));
+                if (rep > 0) ms_sum += ms;  // first run warms up
+            }
+            if (ms_sum < best_ms) {
+                best_ms = ms_sum;
+                best    = v;
+            }
+        }
+        h->tuned[key] = best;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
     });
 }
 

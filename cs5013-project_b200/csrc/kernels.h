@@ -37,7 +37,8 @@ struct SearchArgs {
     uint32_t*       status;
 };
 
-cudaError_t launch_search(const SearchArgs& a, int store, int num_sms, cudaStream_t st);
+cudaError_t launch_search(const SearchArgs& a, int store, int num_sms, cudaStream_t st, int variant = 0);
+int         search_variants();
 size_t      search_smem_per_warp(uint32_t L, uint32_t R, bool rerank);
 
 // RobustPrune over candidates A (expansion list or reverse entries) merged with

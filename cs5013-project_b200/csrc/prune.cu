@@ -38,7 +38,7 @@ struct PruneLayout {
     }
 };
 
-template <int NCH>
+template <int DC>
 __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, uint32_t warp_bytes) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t lane = threadIdx.x & 31u;
@@ -76,8 +76,8 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
             const uint32_t w    = w0 + src;
             const uint32_t node = __shfl_sync(0xffffffffu, mynode, src);
 
-            Query<NCH> nv;
-            load_query<NCH>(nv, a.vecs + (uint64_t)node * a.D, a.D, lane);
+            Query<StoreF32, DC> nv;
+            load_query<StoreF32, DC>(nv, a.vecs + (uint64_t)node * a.D, a.D, lane);
 
             // --- candidates: A then B
             uint32_t nA = 0, aoff = 0;
@@ -109,13 +109,13 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
             __syncwarp();
             // distances to the node for the reverse sources and B
             const uint32_t dstart = rev ? 0u : nA;
-            constexpr int  G      = StoreF32::kGroup;
+            constexpr int  G      = Layout<StoreF32, DC>::kG;
             for (uint32_t g0 = dstart; g0 < nc; g0 += G) {
                 int      gc = (int)min((uint32_t)G, nc - g0);
-                float    y  = dist_group<StoreF32, NCH>(nv, a.vecs, nullptr,
-                                                        [&](int j) { return cid[g0 + j]; }, gc, a.D, lane);
-                uint32_t vi = group_slot_of_lane<G>(lane);
-                if (group_writer<G>(lane) && (int)vi < gc) cd[g0 + vi] = y;
+                float    y  = dist_group<StoreF32, DC>(nv, a.vecs, nullptr,
+                                                       [&](int j) { return cid[g0 + j]; }, gc, a.D, lane);
+                uint32_t vi = round_row_of_lane<StoreF32, DC>(lane);
+                if (round_writer<StoreF32, DC>(lane) && (int)vi < gc) cd[g0 + vi] = y;
             }
             __syncwarp();
             uint32_t ns = 32;
@@ -157,8 +157,8 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
                 __syncwarp();
                 if (ndeg >= R) break;
 
-                Query<NCH> pv;
-                load_query<NCH>(pv, a.vecs + (uint64_t)ps * a.D, a.D, lane);
+                Query<StoreF32, DC> pv;
+                load_query<StoreF32, DC>(pv, a.vecs + (uint64_t)ps * a.D, a.D, lane);
                 for (uint32_t c0 = first; c0 < ncap; c0 += 32) {
                     uint32_t i    = c0 + lane;
                     bool     need = false;
@@ -173,10 +173,10 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
                     __syncwarp();
                     for (uint32_t g0 = 0; g0 < nm; g0 += G) {
                         int      gc = (int)min((uint32_t)G, nm - g0);
-                        float    y  = dist_group<StoreF32, NCH>(
+                        float    y  = dist_group<StoreF32, DC>(
                             pv, a.vecs, nullptr, [&](int j) { return sid[plist[g0 + j]]; }, gc, a.D, lane);
-                        uint32_t vi = group_slot_of_lane<G>(lane);
-                        if (group_writer<G>(lane) && (int)vi < gc) {
+                        uint32_t vi = round_row_of_lane<StoreF32, DC>(lane);
+                        if (round_writer<StoreF32, DC>(lane) && (int)vi < gc) {
                             uint32_t t = plist[g0 + vi];
                             if (y * a.alpha <= key_dist(keys[t])) st[t] = (uint8_t)(kPruned | (st[t] & kFromA));
                         }
@@ -203,11 +203,11 @@ cudaError_t launch_prune(const PruneArgs& a, int num_sms, cudaStream_t st) {
     size_t      smem  = (size_t)lay.bytes * warps;
     void (*kern)(PruneArgs, uint32_t, uint32_t);
     if (a.D <= 128)
-        kern = prune_kernel<1>;
+        kern = prune_kernel<0>;
     else if (a.D <= 256)
-        kern = prune_kernel<2>;
+        kern = prune_kernel<1>;
     else
-        kern = prune_kernel<4>;
+        kern = prune_kernel<2>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;

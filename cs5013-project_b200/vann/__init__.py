@@ -30,7 +30,7 @@ NONE_ID = 0xFFFFFFFF
 EXPORTS = [
     "vann_status_string", "vann_last_error", "vann_abi_version", "vann_create", "vann_destroy",
     "vann_get_info", "vann_load_graph", "vann_save_graph", "vann_set_graph", "vann_get_graph",
-    "vann_build", "vann_search", "vann_search_stats", "vann_sync", "vann_insert", "vann_delete", "vann_delete_by_vector",
+    "vann_build", "vann_search", "vann_search_stats", "vann_autotune", "vann_sync", "vann_insert", "vann_delete", "vann_delete_by_vector",
     "vann_consolidate",
 ]
 
@@ -83,6 +83,7 @@ def lib():
             "vann_build": (C.c_int, [vp, vp, u64, u64, u64, u32, vp]),
             "vann_search": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp, vp]),
             "vann_search_stats": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp, vp, vp, vp, vp]),
+            "vann_autotune": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp]),
             "vann_sync": (C.c_int, [vp, vp]),
             "vann_insert": (C.c_int, [vp, vp, u64, vp, vp]),
             "vann_delete": (C.c_int, [vp, vp, u64, vp]),
@@ -211,6 +212,14 @@ class Index:
                                        C.c_void_p(st[0].data_ptr()), C.c_void_p(st[1].data_ptr()),
                                        C.c_void_p(st[2].data_ptr()), _stream_ptr(stream)))
         return ids, dists, st
+
+    def autotune(self, queries, k: int, L: int, store: str = "f32", rerank: bool = False, quirks: int = 0,
+                 stream=None):
+        """Pick the fastest compiled search variant for (store, rerank, L) on these queries."""
+        torch = _torch()
+        sp = SearchParams(L, k, STORES[store], int(rerank), quirks, 0)
+        _check(lib().vann_autotune(self._h, _dev(queries, torch.float32), queries.shape[0], C.byref(sp),
+                                   _stream_ptr(stream)))
 
     def sync(self, stream=None):
         _check(lib().vann_sync(self._h, _stream_ptr(stream)))

@@ -130,6 +130,12 @@ vann_status vann_search_stats(vann_index* index, const float* d_queries, uint64_
                               const vann_search_params* sp, uint32_t* d_ids, float* d_dists,
                               uint32_t* d_hops, uint32_t* d_evals, uint32_t* d_adj_words,
                               void* stream);
+/* Autotuner: times every compiled launch variant of the search kernel for this
+ * (store, rerank, L) on the given queries (device time, CUDA events on
+ * `stream`) and makes the fastest one the index's choice for later
+ * vann_search calls with the same store, rerank and L.  Synchronises. */
+vann_status vann_autotune(vann_index* index, const float* d_queries, uint64_t nq,
+                          const vann_search_params* sp, void* stream);
 /* Device status word of earlier asynchronous calls: synchronises `stream`,
  * returns VANN_ERR_HOP_LIMIT if a search hit its hop cap since the last call,
  * and clears it. */

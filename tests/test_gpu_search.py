@@ -139,3 +139,18 @@ def test_hop_limit_reported(oracle, vann_mod, graph64):
         idx.sync()
     assert e.value.status == vann_mod.ERR_HOP_LIMIT
     idx.sync()  # cleared
+
+
+def test_autotuned_variant_is_still_exact(oracle, vann_mod, graph64):
+    import torch
+
+    base, g, entry = graph64
+    q = workload.mixture(256, 128, 40, seed=94)
+    idx = _gpu_index(vann_mod, base, g, entry, stores=("f32", "u8"))
+    qd = torch.from_numpy(q).cuda()
+    st, oids, od, _, _ = g.search(q, 48, 10, entry)
+    for store in ("f32", "u8"):
+        idx.autotune(qd, k=10, L=48, store=store)
+        ids, d = idx.search(qd, k=10, L=48, store=store)
+        assert np.array_equal(ids.cpu().numpy().view(np.uint32), oids)
+        assert np.array_equal(d.cpu().numpy(), od)
