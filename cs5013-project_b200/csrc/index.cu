@@ -103,6 +103,8 @@ constexpr int kCounterRing = 256;
 
 }  // namespace
 
+void vann::set_last_error(const char* msg) { set_err(msg); }
+
 struct vann_index {
     vann_params p{};
     int         device  = 0;
@@ -538,6 +540,20 @@ vann_status vann_build(vann_index* h, const float* d_vecs, uint64_t n, uint64_t 
         }
         VCHECK(cudaStreamSynchronize(st));
         VCHECK(cudaGetLastError());
+    });
+}
+
+vann_status vann_build_loaded(vann_index* h, void* stream) {
+    return guard([&] {
+        VREQUIRE(h, VANN_ERR_INVALID, "null argument");
+        VREQUIRE(h->size > 0 && h->entry < h->size, VANN_ERR_STATE, "load or set a graph first");
+        cudaStream_t st = S(stream);
+        const bool   parity = (h->p.flags & VANN_QUIRK_SKIP_BATCH_INDEX) != 0;
+        h->consistent = false;
+        h->nodes.ensure(sizeof(uint32_t) * h->size);
+        VCHECK(vann::launch_iota(h->nodes.as<uint32_t>(), h->size, 0, st));
+        h->vamana_batch(h->nodes.as<uint32_t>(), h->size, h->vecs, parity ? 1u : 2u, 0u, true, st);
+        VCHECK(cudaStreamSynchronize(st));
     });
 }
 

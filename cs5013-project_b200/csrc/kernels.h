@@ -8,6 +8,9 @@
 
 namespace vann {
 
+// message for vann_last_error() on this host thread
+void set_last_error(const char* msg);
+
 struct SearchArgs {
     const void*     store;     // traversal copy (F32 / BF16 / FP8 / U8 rows)
     const float*    scale;     // per-row scale of the FP8 copy

@@ -30,7 +30,7 @@ NONE_ID = 0xFFFFFFFF
 EXPORTS = [
     "vann_status_string", "vann_last_error", "vann_abi_version", "vann_create", "vann_destroy",
     "vann_get_info", "vann_load_graph", "vann_save_graph", "vann_set_graph", "vann_get_graph",
-    "vann_build", "vann_search", "vann_search_stats", "vann_autotune", "vann_sync", "vann_insert", "vann_delete", "vann_delete_by_vector",
+    "vann_build", "vann_build_loaded", "vann_search", "vann_search_stats", "vann_autotune", "vann_sync", "vann_insert", "vann_delete", "vann_delete_by_vector",
     "vann_consolidate",
 ]
 
@@ -81,6 +81,7 @@ def lib():
             "vann_set_graph": (C.c_int, [vp, vp, vp, vp, u64, u32, u32]),
             "vann_get_graph": (C.c_int, [vp, vp, vp, vp]),
             "vann_build": (C.c_int, [vp, vp, u64, u64, u64, u32, vp]),
+            "vann_build_loaded": (C.c_int, [vp, vp]),
             "vann_search": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp, vp]),
             "vann_search_stats": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp, vp, vp, vp, vp]),
             "vann_autotune": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp]),
@@ -183,6 +184,10 @@ class Index:
         torch = _torch()
         _check(lib().vann_build(self._h, _dev(vecs, torch.float32), vecs.shape[0], batch, seed,
                                 NONE_ID if entry is None else entry, _stream_ptr(stream)))
+
+    def build_loaded(self, stream=None):
+        """Reference build over the graph already loaded (its adjacency is the start graph)."""
+        _check(lib().vann_build_loaded(self._h, _stream_ptr(stream)))
 
     def search(self, queries, k: int, L: int, store: str = "f32", rerank: bool = False,
                quirks: int = 0, max_hops: int = 0, out=None, stream=None):

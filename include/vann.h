@@ -118,6 +118,12 @@ vann_status vann_get_graph(vann_index* index, float* h_vecs, uint32_t* h_deg, ui
 vann_status vann_build(vann_index* index, const float* d_vecs, uint64_t n, uint64_t batch,
                        uint64_t seed, uint32_t entry, void* stream);
 
+/* runVamana over the graph already in the index (vann_load_graph /
+ * vann_set_graph): the loaded adjacency is the start graph, exactly as the
+ * reference builds over the random graph it reads (vamana_impl.cuh:289-360,
+ * utils.cuh:113-148).  One batch over every node.  Synchronises `stream`. */
+vann_status vann_build_loaded(vann_index* index, void* stream);
+
 /* Vamana<T>::searchPoints (vamana/include/vamana_impl.cuh:55-96, GreedySearch
  * search.cuh:226-367).  d_queries: nq x dim FP32.  Writes nq x k ids / squared
  * L2 distances, padded with UINT32_MAX / +inf.  Asynchronous on `stream`. */

@@ -132,3 +132,25 @@ def test_save_load_roundtrip(vann_mod, tmp_path):
     assert np.array_equal(va, vb) and np.array_equal(da, db)
     for i in range(1500):
         assert np.array_equal(aa[i, :da[i]], ab[i, :db[i]])
+
+
+def test_build_over_loaded_start_graph(oracle, vann_mod):
+    """runVamana over a start graph read from the caller (the reference reads one
+    from sift10k_randomgraph.bin): the loaded adjacency, duplicates included, is
+    the start graph."""
+    import torch  # noqa: F401
+
+    n, R, L = 3000, 64, 100
+    base = workload.mixture(n, 128, 30, seed=39)
+    rng = np.random.default_rng(5)
+    adj = rng.integers(0, n, (n, R)).astype(np.uint32)  # with duplicates, like the reference's file
+    deg = np.full(n, R, np.uint32)
+    entry = 1500
+    og = oracle.Graph(base, deg.copy(), adj.copy())
+    assert og.vamana_batch(0, n, L, 1.5, entry, 600, 500, skip_mode=1,
+                           bloom_mode=oracle.BLOOM_SNAPSHOT) == 0
+    idx = vann_mod.Index(128, R, L, 1.5, capacity=n, quirks=vann_mod.QUIRK_SKIP_BATCH_INDEX)
+    idx.set_graph(base, deg, adj, entry)
+    idx.build_loaded()
+    _, gdeg, gadj = idx.get_graph()
+    assert _rows_equal(gdeg, gadj, og.deg, og.adj) == []
