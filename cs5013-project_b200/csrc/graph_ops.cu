@@ -4,6 +4,9 @@
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 
+#include <mutex>
+
+#include "../../include/vann.h"
 #include "common.cuh"
 #include "kernels.h"
 
@@ -291,3 +294,80 @@ cudaError_t launch_consolidate_candidates(const uint32_t* deg, const uint32_t* a
 }
 
 }  // namespace vann
+
+// ---------------------------------------------------------------- allocation-free medoid
+// Entry-point selection (the medoid above) for callers that must not allocate
+// device memory.  Its scratch -- the D column sums (FP64) and the argmin word
+// pair -- lives in this file-scope device array instead of memory the library
+// would cudaMalloc: up to kNoAllocMaxDim dimensions, 32 KiB + 256 B, held by
+// every device that loads the library until the process exits.
+namespace {
+constexpr uint32_t kNoAllocMaxDim = 4096;
+constexpr size_t   kNoAllocSumBytes = sizeof(double) * kNoAllocMaxDim;
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocSumBytes + 256];
+
+__global__ void medoid_result_kernel(const unsigned long long* best, uint32_t* out) {
+    *out = (uint32_t)best[1];
+}
+
+// device address of g_noalloc_scratch per device, resolved once per device
+std::mutex g_noalloc_mu;
+void*      g_noalloc_addr[256] = {};
+}  // namespace
+
+extern "C" vann_status vann_medoid_noalloc(const float* d_vecs, uint64_t n, uint32_t dim,
+                                           uint32_t* d_medoid_out, void* stream) {
+    if (d_vecs == nullptr || d_medoid_out == nullptr || n == 0 || dim == 0) {
+        vann::set_last_error("vann_medoid_noalloc: null pointer or empty input");
+        return VANN_ERR_INVALID;
+    }
+    if (dim > kNoAllocMaxDim) {
+        vann::set_last_error("vann_medoid_noalloc: dim exceeds the fixed scratch maximum of 4096");
+        return VANN_ERR_UNSUPPORTED;
+    }
+    if (n >= 0xffffffffull) {
+        vann::set_last_error("vann_medoid_noalloc: n must be below 2^32");
+        return VANN_ERR_UNSUPPORTED;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) {
+        vann::set_last_error("vann_medoid_noalloc: no current CUDA device");
+        return VANN_ERR_CUDA;
+    }
+    void* base = nullptr;
+    {
+        // set-up on the first call on this device (with the device current):
+        // the host-side symbol is only a stand-in, the kernels need the device
+        // address, which cudaGetSymbolAddress resolves here
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (g_noalloc_addr[dev] == nullptr) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) {
+                vann::set_last_error("vann_medoid_noalloc: cudaGetSymbolAddress failed");
+                return VANN_ERR_CUDA;
+            }
+            g_noalloc_addr[dev] = p;
+        }
+        base = g_noalloc_addr[dev];
+    }
+    cudaStream_t        st   = static_cast<cudaStream_t>(stream);
+    double*             sums = static_cast<double*>(base);
+    unsigned long long* best = reinterpret_cast<unsigned long long*>(static_cast<char*>(base) + kNoAllocSumBytes);
+    // the array keeps the previous call's contents: clear what must start fresh
+    if (cudaMemsetAsync(sums, 0, sizeof(double) * dim, st) != cudaSuccess ||
+        cudaMemsetAsync(best, 0xff, 2 * sizeof(unsigned long long), st) != cudaSuccess) {
+        vann::set_last_error("vann_medoid_noalloc: clearing the scratch failed");
+        return VANN_ERR_CUDA;
+    }
+    dim3 g((unsigned)((n + 1023) / 1024), (dim + 127) / 128);
+    vann::col_sum_kernel<<<g, 128, 0, st>>>(d_vecs, n, dim, sums);
+    vann::medoid_dist_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_vecs, n, dim, sums, best, 0);
+    vann::medoid_dist_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_vecs, n, dim, sums, best, 1);
+    medoid_result_kernel<<<1, 1, 0, st>>>(best, d_medoid_out);
+    if (cudaGetLastError() != cudaSuccess) {
+        vann::set_last_error("vann_medoid_noalloc: kernel launch failed");
+        return VANN_ERR_CUDA;
+    }
+    return VANN_OK;
+}
+

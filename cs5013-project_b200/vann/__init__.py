@@ -31,7 +31,7 @@ EXPORTS = [
     "vann_status_string", "vann_last_error", "vann_abi_version", "vann_create", "vann_destroy",
     "vann_get_info", "vann_load_graph", "vann_save_graph", "vann_set_graph", "vann_get_graph",
     "vann_build", "vann_build_loaded", "vann_search", "vann_search_stats", "vann_autotune", "vann_sync", "vann_insert", "vann_delete", "vann_delete_by_vector",
-    "vann_consolidate",
+    "vann_consolidate", "vann_medoid_noalloc",
 ]
 
 
@@ -90,6 +90,7 @@ def lib():
             "vann_delete": (C.c_int, [vp, vp, u64, vp]),
             "vann_delete_by_vector": (C.c_int, [vp, vp, u64, vp, vp]),
             "vann_consolidate": (C.c_int, [vp, vp]),
+            "vann_medoid_noalloc": (C.c_int, [vp, u64, u32, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -251,6 +252,14 @@ class Index:
 
     def consolidate(self, stream=None):
         _check(lib().vann_consolidate(self._h, _stream_ptr(stream)))
+
+
+def medoid_noalloc(vecs, out, stream=None):
+    """Entry point (medoid) of the rows of `vecs` written into the 1-element int32
+    tensor `out`, allocating no device memory (vann_medoid_noalloc)."""
+    torch = _torch()
+    _check(lib().vann_medoid_noalloc(_dev(vecs, torch.float32), vecs.shape[0], vecs.shape[1],
+                                     _dev(out, torch.int32), _stream_ptr(stream)))
 
 
 class Vamana:
