@@ -199,9 +199,10 @@ def main():
                 return L
         return sweep[name][-1][0]
 
+    tune_ms = {}
     for store, rr in forms:
         name = store + ("+rerank" if rr else "")
-        idx.autotune(q_d, k=K, L=op_point0(name), store=store, rerank=rr)
+        tune_ms[name] = idx.autotune(q_d, k=K, L=op_point0(name), store=store, rerank=rr)
 
     def op_point(name):
         for L, r in sweep[name]:
@@ -305,6 +306,7 @@ def main():
             "forms": {nm: {"L": v["L"], "recall@10": round(v["recall"], 4), "qps": round(qps(nm), 1),
                            "p99_ms": round(float(np.percentile(v["ms"], 99)), 4)} for nm, v in results.items()},
             "speedup_vs_fp32_plain": round(qps(head) / qps("f32"), 3),
+            "autotune_ms_per_variant": tune_ms,
             "sweep": {nm: [[L, round(r, 4)] for L, r in v] for nm, v in sweep.items()},
             "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": nq * DIM * 4,
                     "d2h_bytes_per_step": nq * K * 8},

@@ -22,7 +22,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-ccbin", "g++
          "--expt-relaxed-constexpr", "-Wno-deprecated-gpu-targets"]
 SOURCES = ["search.cu", "search_f32.cu", "search_bf16.cu", "search_fp8.cu", "search_u8.cu", "prune.cu",
            "graph_ops.cu", "index.cu"]
-HEADERS = ["common.cuh", "kernels.h", "search_impl.cuh"]
+HEADERS = ["common.cuh", "kernels.h", "search_impl.cuh", "search_reg.cuh", "search_dispatch.cuh"]
 
 
 def _stale(obj: str, src: str) -> bool:

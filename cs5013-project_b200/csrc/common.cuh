@@ -136,10 +136,13 @@ __device__ __forceinline__ uint4 load16(const void* base, uint64_t row_bytes, ui
 // [0, 255] (uint8 rows then use exact dp4a integer arithmetic).
 template <typename S, int DC>
 struct Query {
-    float    f[Layout<S, DC>::kCPL][S::kElems];
-    uint32_t u[Layout<S, DC>::kCPL][S::kElems / 4];
-    int      qq;
-    bool     qint;
+    // FP32 copy of the lane's chunks (integer stores keep none: their rare
+    // non-integer fallback re-reads the row through L1)
+    float        f[S::kInt ? 1 : Layout<S, DC>::kCPL][S::kInt ? 1 : S::kElems];
+    uint32_t     u[Layout<S, DC>::kCPL][S::kElems / 4];
+    const float* row;
+    int          qq;
+    bool         qint;
 };
 
 template <typename S, int DC>
@@ -161,8 +164,8 @@ __device__ __forceinline__ void load_query(Query<S, DC>& q, const float* row, ui
             uint32_t pk = 0;
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                q.f[c][4 * v + i] = e[i];
-                bool good         = e[i] >= 0.f && e[i] <= 255.f && rintf(e[i]) == e[i];
+                if constexpr (!S::kInt) q.f[c][4 * v + i] = e[i];
+                bool good = e[i] >= 0.f && e[i] <= 255.f && rintf(e[i]) == e[i];
                 ok &= good;
                 uint32_t b = good ? (uint32_t)e[i] : 0u;
                 pk |= b << (8 * i);
@@ -171,6 +174,7 @@ __device__ __forceinline__ void load_query(Query<S, DC>& q, const float* row, ui
             q.u[c][v] = pk;
         }
     }
+    q.row  = row;
     q.qint = __all_sync(0xffffffffu, ok);
     // each group of T lanes holds the whole query
 #pragma unroll
@@ -278,10 +282,26 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
         float e[M][S::kElems];
 #pragma unroll
         for (int m = 0; m < M; ++m) S::widen(x[m][c], sc[m], e[m]);
+        float qf[S::kElems];
+        if constexpr (S::kInt) {
+            const uint32_t k = t + (uint32_t)Ly::kT * c;
+#pragma unroll
+            for (int v4 = 0; v4 < S::kElems / 4; ++v4) {
+                float4 z = k < chunks ? __ldg(reinterpret_cast<const float4*>(q.row + k * S::kElems) + v4)
+                                      : make_float4(0.f, 0.f, 0.f, 0.f);
+                qf[4 * v4] = z.x;
+                qf[4 * v4 + 1] = z.y;
+                qf[4 * v4 + 2] = z.z;
+                qf[4 * v4 + 3] = z.w;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < S::kElems; ++i) qf[i] = q.f[c][i];
+        }
 #pragma unroll
         for (int i = 0; i < S::kElems; ++i) {
 #pragma unroll
-            for (int m = 0; m < M; ++m) v[m] = sqdiff(q.f[c][i], e[m][i], v[m]);
+            for (int m = 0; m < M; ++m) v[m] = sqdiff(qf[i], e[m][i], v[m]);
         }
     }
     return group_reduce<M, Ly::kT, float>(v, lane);

@@ -598,8 +598,10 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
     });
 }
 
+int vann_search_variant_count(void) { return vann::search_variants(); }
+
 vann_status vann_autotune(vann_index* h, const float* d_queries, uint64_t nq, const vann_search_params* sp,
-                          void* stream) {
+                          float* h_ms_out, void* stream) {
     return guard([&] {
         VREQUIRE(h && sp && d_queries && nq > 0, VANN_ERR_INVALID, "null argument");
         cudaStream_t st = S(stream);
@@ -625,6 +627,7 @@ vann_status vann_autotune(vann_index* h, const float* d_queries, uint64_t nq, co
                 VCHECK(cudaEventElapsedTime(&ms, e0, e1));
                 if (rep > 0) ms_sum += ms;  // first run warms up
             }
+            if (h_ms_out) h_ms_out[v] = ms_sum / 3.f;
             if (ms_sum < best_ms) {
                 best_ms = ms_sum;
                 best    = v;

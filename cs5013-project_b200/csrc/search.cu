@@ -1,6 +1,6 @@
 // search.cu -- dispatch of the search kernel by row format; the kernel itself
 // is in search_impl.cuh, instantiated once per format in search_<format>.cu.
-#include "search_impl.cuh"
+#include "search_dispatch.cuh"
 
 namespace vann {
 

@@ -1,0 +1,62 @@
+// search_dispatch.cuh -- picks the search kernel instantiation for a launch:
+// register worklist (search_reg.cuh) for L <= 64 at D <= 128 and R <= 64,
+// shared-memory worklist (search_impl.cuh) otherwise, and the launch-bound
+// variant chosen by the autotuner.
+#pragma once
+#include "search_reg.cuh"
+
+namespace vann {
+
+// Launch-bound variants (minimum resident blocks per SM, i.e. a register cap)
+// exist for the common shape (D <= 128, R <= 64); the autotuner picks one.
+constexpr int kSearchVariants = 5;
+
+template <typename S, int DC, int SPL>
+static cudaError_t launch_v(const SearchArgs& a, int variant, int sms, cudaStream_t st) {
+    if constexpr (DC == 0 && SPL <= 2) {
+        // worklist in registers for L <= 64
+        if (a.L <= 32) {
+            switch (variant) {
+                case 1: return launch_rw<S, DC, SPL, 1, 4>(a, sms, st);
+                case 2: return launch_rw<S, DC, SPL, 1, 5>(a, sms, st);
+                case 3: return launch_rw<S, DC, SPL, 1, 7>(a, sms, st);
+                case 4: return launch_rw<S, DC, SPL, 1, 8>(a, sms, st);
+                default: return launch_rw<S, DC, SPL, 1, 6>(a, sms, st);
+            }
+        }
+        if (a.L <= 64) {
+            switch (variant) {
+                case 1: return launch_rw<S, DC, SPL, 2, 4>(a, sms, st);
+                case 2: return launch_rw<S, DC, SPL, 2, 5>(a, sms, st);
+                case 3: return launch_rw<S, DC, SPL, 2, 7>(a, sms, st);
+                case 4: return launch_rw<S, DC, SPL, 2, 8>(a, sms, st);
+                default: return launch_rw<S, DC, SPL, 2, 6>(a, sms, st);
+            }
+        }
+        switch (variant) {
+            case 1: return launch_t<S, DC, SPL, 4>(a, sms, st);
+            case 2: return launch_t<S, DC, SPL, 5>(a, sms, st);
+            case 3: return launch_t<S, DC, SPL, 7>(a, sms, st);
+            case 4: return launch_t<S, DC, SPL, 8>(a, sms, st);
+            default: break;
+        }
+    }
+    return launch_t<S, DC, SPL, 6>(a, sms, st);
+}
+
+template <typename S, int DC>
+static cudaError_t launch_r(const SearchArgs& a, int variant, int sms, cudaStream_t st) {
+    if (a.R <= 32) return launch_v<S, DC, 1>(a, variant, sms, st);
+    if (a.R <= 64) return launch_v<S, DC, 2>(a, variant, sms, st);
+    return launch_v<S, DC, 4>(a, variant, sms, st);
+}
+
+template <typename S>
+static cudaError_t launch_store(const SearchArgs& a, int variant, int sms, cudaStream_t st) {
+    if (a.D % S::kElems != 0) return cudaErrorInvalidValue;
+    if (a.D <= 128) return launch_r<S, 0>(a, variant, sms, st);
+    if (a.D <= 256) return launch_r<S, 1>(a, variant, sms, st);
+    return launch_r<S, 2>(a, variant, sms, st);
+}
+
+}  // namespace vann

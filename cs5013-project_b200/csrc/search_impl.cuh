@@ -105,6 +105,21 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
         __syncwarp();
         uint32_t n = 1, parent = entry, ppos = 0, hops = 0, nv = 0, evals = 1, adjw = 0;
         float    pd = d0;
+        // the parent's degree, adjacency row and filter slots, loaded in one round
+        // trip; from the second hop on they are prefetched before the merge
+        uint32_t nid[SPL], hp[SPL], dg;
+        auto     fetch_row = [&](uint32_t node) {
+            const uint32_t* row  = a.adj + (uint64_t)node * R;
+            const uint32_t* rowh = a.adj_h + (uint64_t)node * R;
+#pragma unroll
+            for (int s = 0; s < SPL; ++s) {
+                uint32_t j = (uint32_t)s * 32u + lane;
+                nid[s]     = j < R ? __ldg(row + j) : 0u;
+                hp[s]      = j < R ? __ldg(rowh + j) : 0u;
+            }
+            dg = __ldg(a.deg + node);
+        };
+        fetch_row(parent);
 
         for (;;) {
             if (hops >= a.max_hops) {
@@ -119,18 +134,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
                 }
                 ++nv;
             }
-            // degree and adjacency row in one round trip
-            const uint32_t* row  = a.adj + (uint64_t)parent * R;
-            const uint32_t* rowh = a.adj_h + (uint64_t)parent * R;
-            uint32_t        nid[SPL], hp[SPL];
-#pragma unroll
-            for (int s = 0; s < SPL; ++s) {
-                uint32_t j = (uint32_t)s * 32u + lane;
-                nid[s]     = j < R ? __ldg(row + j) : 0u;
-                hp[s]      = j < R ? __ldg(rowh + j) : 0u;
-            }
-            uint32_t dg = __ldg(a.deg + parent);
-            dg          = dg < R ? dg : R;
+            dg = dg < R ? dg : R;
             adjw += dg;
 
             // filterNeighbors: every slot checks the filter as it stood before this
@@ -232,6 +236,33 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
                 }
                 __syncwarp();
 
+            }
+
+            // next parent, decided before the merge: the first unvisited entry of the
+            // merged list is either the best kept candidate or the first unvisited
+            // existing entry after the current parent, whichever is closer (existing
+            // first on equal distance).  Its row is fetched now so the load overlaps
+            // the merge.
+            uint32_t e_pos = kNone;
+            for (uint32_t c0 = ppos + 1u; c0 < n; c0 += 32u) {
+                uint32_t i  = c0 + lane;
+                bool     uv = i < n && !(wl_id[i] & kVisitedBit);
+                uint32_t m  = __ballot_sync(0xffffffffu, uv);
+                if (m) {
+                    e_pos = c0 + __ffs(m) - 1u;
+                    break;
+                }
+            }
+            const float    d_e      = e_pos != kNone ? wl_d[e_pos] : __int_as_float(0x7f800000);
+            const bool     take_new = kc > 0 && nb_d[0] < d_e;
+            const bool     has_next = take_new || e_pos != kNone;
+            const uint32_t next     = take_new ? nb_id[0] : (has_next ? (wl_id[e_pos] & ~kVisitedBit) : 0u);
+            const float    next_d   = take_new ? nb_d[0] : d_e;
+            if (has_next) fetch_row(next);
+            __syncwarp();
+
+            uint32_t p0 = L;
+            if (kc > 0) {
                 // mergeIntoWorklist: new entry j lands at j + #(existing <= d_j);
                 // existing entry i moves to i + #(new < d_i); keep the first L
                 uint32_t pj[SPL];
@@ -240,7 +271,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
                     uint32_t j = (uint32_t)s * 32u + lane;
                     pj[s]      = j < kc ? j + upper_bound_f(wl_d, n, nb_d[j]) : L;
                 }
-                uint32_t p0 = __shfl_sync(0xffffffffu, pj[0], 0);
+                p0 = __shfl_sync(0xffffffffu, pj[0], 0);
                 if (p0 < L) {
                     if (p0 < n) {
                         uint32_t nchunks = (n - p0 + 31u) >> 5;
@@ -270,28 +301,14 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
                         }
                     }
                     n = min(n + kc, L);
-                    if (p0 < ppos + 1u) ppos = p0 - 1u;  // rescan from p0
                 }
                 __syncwarp();
             }
 
-            // next parent: first unvisited entry
-            uint32_t start = ppos + 1u;
-            int      found = -1;
-            for (uint32_t c0 = start; c0 < n; c0 += 32u) {
-                uint32_t i  = c0 + lane;
-                bool     uv = i < n && !(wl_id[i] & kVisitedBit);
-                uint32_t m  = __ballot_sync(0xffffffffu, uv);
-                if (m) {
-                    found = (int)(c0 + __ffs(m) - 1);
-                    break;
-                }
-            }
-            if (found < 0) break;
-            ppos   = (uint32_t)found;
-            parent = wl_id[ppos];
-            pd     = wl_d[ppos];
-            __syncwarp();
+            if (!has_next) break;
+            ppos   = take_new ? p0 : e_pos;
+            parent = next;
+            pd     = next_d;
             if (lane == 0) wl_id[ppos] = parent | kVisitedBit;
             __syncwarp();
         }
@@ -356,6 +373,10 @@ static cudaError_t launch_t(const SearchArgs& a, int num_sms, cudaStream_t st) {
     auto       kern  = search_kernel<S, DC, SPL, MINB>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    // per-query bloom filters dominate shared memory: take the whole carveout
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
     if (e != cudaSuccess) return e;
@@ -366,34 +387,6 @@ static cudaError_t launch_t(const SearchArgs& a, int num_sms, cudaStream_t st) {
     if (grid == 0) return cudaSuccess;
     kern<<<(unsigned)grid, warps * 32, smem, st>>>(a);
     return cudaGetLastError();
-}
-
-// Launch-bound variants (minimum resident blocks per SM, i.e. a register cap)
-// exist for the common shape (D <= 128, R <= 64); the autotuner picks one.
-constexpr int kSearchVariants = 3;
-
-template <typename S, int DC, int SPL>
-static cudaError_t launch_v(const SearchArgs& a, int variant, int sms, cudaStream_t st) {
-    if constexpr (DC == 0 && SPL <= 2) {
-        if (variant == 1) return launch_t<S, DC, SPL, 4>(a, sms, st);
-        if (variant == 2) return launch_t<S, DC, SPL, 8>(a, sms, st);
-    }
-    return launch_t<S, DC, SPL, 6>(a, sms, st);
-}
-
-template <typename S, int DC>
-static cudaError_t launch_r(const SearchArgs& a, int variant, int sms, cudaStream_t st) {
-    if (a.R <= 32) return launch_v<S, DC, 1>(a, variant, sms, st);
-    if (a.R <= 64) return launch_v<S, DC, 2>(a, variant, sms, st);
-    return launch_v<S, DC, 4>(a, variant, sms, st);
-}
-
-template <typename S>
-static cudaError_t launch_store(const SearchArgs& a, int variant, int sms, cudaStream_t st) {
-    if (a.D % S::kElems != 0) return cudaErrorInvalidValue;
-    if (a.D <= 128) return launch_r<S, 0>(a, variant, sms, st);
-    if (a.D <= 256) return launch_r<S, 1>(a, variant, sms, st);
-    return launch_r<S, 2>(a, variant, sms, st);
 }
 
 }  // namespace vann

@@ -30,7 +30,7 @@ NONE_ID = 0xFFFFFFFF
 EXPORTS = [
     "vann_status_string", "vann_last_error", "vann_abi_version", "vann_create", "vann_destroy",
     "vann_get_info", "vann_load_graph", "vann_save_graph", "vann_set_graph", "vann_get_graph",
-    "vann_build", "vann_build_loaded", "vann_search", "vann_search_stats", "vann_autotune", "vann_sync", "vann_insert", "vann_delete", "vann_delete_by_vector",
+    "vann_build", "vann_build_loaded", "vann_search", "vann_search_stats", "vann_autotune", "vann_search_variant_count", "vann_sync", "vann_insert", "vann_delete", "vann_delete_by_vector",
     "vann_consolidate", "vann_medoid_noalloc",
 ]
 
@@ -84,7 +84,8 @@ def lib():
             "vann_build_loaded": (C.c_int, [vp, vp]),
             "vann_search": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp, vp]),
             "vann_search_stats": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp, vp, vp, vp, vp]),
-            "vann_autotune": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp]),
+            "vann_autotune": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp]),
+            "vann_search_variant_count": (C.c_int, []),
             "vann_sync": (C.c_int, [vp, vp]),
             "vann_insert": (C.c_int, [vp, vp, u64, vp, vp]),
             "vann_delete": (C.c_int, [vp, vp, u64, vp]),
@@ -224,8 +225,11 @@ class Index:
         """Pick the fastest compiled search variant for (store, rerank, L) on these queries."""
         torch = _torch()
         sp = SearchParams(L, k, STORES[store], int(rerank), quirks, 0)
+        nv = lib().vann_search_variant_count()
+        ms = (C.c_float * nv)()
         _check(lib().vann_autotune(self._h, _dev(queries, torch.float32), queries.shape[0], C.byref(sp),
-                                   _stream_ptr(stream)))
+                                   ms, _stream_ptr(stream)))
+        return [round(float(x), 4) for x in ms]
 
     def sync(self, stream=None):
         _check(lib().vann_sync(self._h, _stream_ptr(stream)))

@@ -141,7 +141,10 @@ vann_status vann_search_stats(vann_index* index, const float* d_queries, uint64_
  * `stream`) and makes the fastest one the index's choice for later
  * vann_search calls with the same store, rerank and L.  Synchronises. */
 vann_status vann_autotune(vann_index* index, const float* d_queries, uint64_t nq,
-                          const vann_search_params* sp, void* stream);
+                          const vann_search_params* sp, float* h_ms_out, void* stream);
+/* Number of compiled search variants (length of vann_autotune's h_ms_out,
+ * which may be NULL; it receives the mean ms of each variant). */
+int vann_search_variant_count(void);
 /* Device status word of earlier asynchronous calls: synchronises `stream`,
  * returns VANN_ERR_HOP_LIMIT if a search hit its hop cap since the last call,
  * and clears it. */
