@@ -56,6 +56,14 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile", action="store_true", help="short run for a profiler capture")
+    ap.add_argument("--config", default="search", choices=["search", "churn", "precision", "serve"],
+                    help="search: the headline line; churn / precision: the FreshVamana churn and "
+                         "reduced-precision configurations (their own JSON lines)")
+    ap.add_argument("--rounds", type=int, default=20)
+    ap.add_argument("--rate", type=float, default=50_000.0, help="serve: offered requests/s")
+    ap.add_argument("--duration", type=float, default=5.0, help="serve: seconds of arrivals")
+    ap.add_argument("--write-frac", type=float, default=0.1, help="serve: share of write requests")
+    ap.add_argument("--max-write", type=int, default=10_000, help="serve: largest write batch")
     return ap.parse_args()
 
 
@@ -112,10 +120,12 @@ def ground_truth(torch, base_d, q_d, k):
     b64 = base_d.double()
     bn = (b64 * b64).sum(1)
     out = []
-    for s in range(0, q_d.shape[0], 512):
-        qq = q_d[s:s + 512].double()
+    chunk = max(1, min(512, int(2e9 // (8 * b64.shape[0]))))  # ~2 GB distance tile
+    for s in range(0, q_d.shape[0], chunk):
+        qq = q_d[s:s + chunk].double()
         d = (qq * qq).sum(1, keepdim=True) + bn[None, :] - 2.0 * qq @ b64.T
         out.append(torch.topk(d, k, dim=1, largest=False).indices)
+        del d
     del b64
     return torch.cat(out).int()
 
@@ -458,7 +468,267 @@ def main_reference():
     return 0
 
 
+def gt_live(torch, vec_by_id, live_ids_d, q_d, k):
+    """FP64 exact kNN over the live rows only; returns their global ids."""
+    base = vec_by_id.index_select(0, live_ids_d)
+    local = ground_truth(torch, base, q_d, k)
+    return live_ids_d[local.long()].int()
+
+
+def main_churn():
+    """FreshVamana churn on the 1M x 128 index: each round lazily deletes 5% of the live
+    ids (uniform), consolidates, then inserts 5% new points in uneven batches of 1k-50k;
+    recall@10 at L=100 over the live points and insert / delete throughput per round."""
+    args = parse()
+    import torch
+
+    import vann
+    from vann import workload
+
+    dev = torch.device("cuda", 0)
+    n, nq, rounds = args.n, args.nq, args.rounds
+    clusters = 1000 if n >= 100_000 else max(10, n // 1000)
+    base = workload.mixture(n, DIM, clusters, seed=1)
+    q = workload.mixture(nq, DIM, clusters, seed=2)
+    q_d = torch.from_numpy(q).to(dev)
+    cap = int(n * 1.1)
+    vec_by_id = torch.zeros((cap, DIM), dtype=torch.float32, device=dev)
+    vec_by_id[:n] = torch.from_numpy(base).to(dev)
+    idx = vann.Index(DIM, R, L_BUILD, ALPHA, capacity=cap)
+    t0 = time.time()
+    idx.build(vec_by_id[:n].contiguous(), batch=BATCH, seed=2024)
+    torch.cuda.synchronize()
+    build_s = time.time() - t0
+    rng = np.random.default_rng(7)
+    live = np.arange(n, dtype=np.int64)
+    out = []
+    for r in range(rounds):
+        ndel = int(0.05 * len(live))
+        dels = rng.choice(live, ndel, replace=False)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        idx.delete(torch.from_numpy(dels.astype(np.int32)).to(dev))
+        idx.consolidate()
+        torch.cuda.synchronize()
+        del_s = time.time() - t0
+        live = np.setdiff1d(live, dels, assume_unique=True)
+        sizes, left = [], ndel
+        while left > 0:
+            s = int(min(left, rng.integers(1000, 50_001)))
+            sizes.append(s)
+            left -= s
+        newv_d = torch.from_numpy(workload.mixture(ndel, DIM, clusters, seed=1000 + r)).to(dev)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        new_ids, off = [], 0
+        for s in sizes:
+            new_ids.append(idx.insert(newv_d[off:off + s].contiguous()))
+            off += s
+        torch.cuda.synchronize()
+        ins_s = time.time() - t0
+        new_ids = torch.cat(new_ids).long()
+        vec_by_id[new_ids] = newv_d
+        live = np.concatenate([live, new_ids.cpu().numpy()])
+        gt = gt_live(torch, vec_by_id, torch.from_numpy(live).to(dev), q_d, K)
+        ids, _ = idx.search(q_d, k=K, L=100)
+        rec = recall(torch, ids, gt)
+        out.append({"round": r + 1, "deleted": ndel, "inserted": ndel, "insert_batches": len(sizes),
+                    "delete_consolidate_s": round(del_s, 3), "deletes_per_s": round(ndel / del_s, 1),
+                    "insert_s": round(ins_s, 3), "inserts_per_s": round(ndel / ins_s, 1),
+                    "recall@10_L100": round(rec, 4), "live": int(len(live)), "index_size": idx.info()["size"]})
+        print(json.dumps(out[-1]), flush=True)
+    line = {"metric": "FreshVamana churn on 1Mx128: recall@10 (L=100) and insert/delete throughput per round",
+            "config": {"workload": f"{n}x{DIM} integer-valued f32, {clusters}-cluster mixture; {nq} queries; "
+                                   f"R={R} L={L_BUILD} alpha={ALPHA}; {rounds} rounds of 5% deletes + "
+                                   f"consolidate + 5% inserts in batches of 1k-50k", "build_s": round(build_s, 2)},
+            "data": "synthetic (seeded clipped Gaussian mixture)",
+            "final_recall@10": out[-1]["recall@10_L100"] if out else None,
+            "min_recall@10": min(o["recall@10_L100"] for o in out) if out else None,
+            "median_inserts_per_s": float(np.median([o["inserts_per_s"] for o in out])) if out else None,
+            "median_deletes_per_s": float(np.median([o["deletes_per_s"] for o in out])) if out else None,
+            "rounds": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main_precision():
+    """Reduced precision on float data: 5M x 96 from a 2,000-cluster mixture with unit-norm
+    centres and sigma 0.05; FP32, BF16+rerank and FP8-E4M3 (per-row scale)+rerank traversal;
+    recall@10 at L in {64, 128}, QPS, and the traversal distance error against FP64."""
+    args = parse()
+    import torch
+
+    import vann
+    from vann import workload
+
+    dev = torch.device("cuda", 0)
+    n = args.n if args.n != N_BASE else 5_000_000
+    nq, D = args.nq, 96
+    base = workload.mixture(n, D, 2000, seed=11, sigma=0.05, integer=False, unit_norm=True)
+    q = workload.mixture(nq, D, 2000, seed=12, sigma=0.05, integer=False, unit_norm=True)
+    base_d = torch.from_numpy(base).to(dev)
+    q_d = torch.from_numpy(q).to(dev)
+    del base
+    idx = vann.Index(D, R, L_BUILD, ALPHA, capacity=n, stores=("f32", "bf16", "fp8"))
+    t0 = time.time()
+    idx.build(base_d, batch=BATCH, seed=2024)
+    torch.cuda.synchronize()
+    build_s = time.time() - t0
+    gt = ground_truth(torch, base_d, q_d, K)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def rel_err(ids, d):
+        x = base_d[ids.clamp(min=0).long()].double()
+        exact = ((x - q_d.double()[:, None, :]) ** 2).sum(-1)
+        return ((d.double() - exact).abs() / exact.clamp(min=1e-30))[ids >= 0]
+
+    res = {}
+    for L in (64, 128):
+        for store, rr in (("f32", False), ("bf16", True), ("fp8", True)):
+            name = f"{store}{'+rerank' if rr else ''}@L{L}"
+            idx.autotune(q_d, k=K, L=L, store=store, rerank=rr)
+            ids, d = idx.search(q_d, k=K, L=L, store=store, rerank=rr)
+            t = time_steps(torch, lambda s=store, rr=rr, L=L: idx.search(q_d, k=K, L=L, store=s, rerank=rr),
+                           args.steps, args.warmup, flush)
+            ent = {"recall@10": round(recall(torch, ids, gt), 4),
+                   "qps": round(nq / (statistics.mean(t) / 1e3), 1),
+                   "returned_max_rel_err": float(rel_err(ids, d).max())}
+            if store != "f32":
+                ids2, d2 = idx.search(q_d, k=K, L=L, store=store, rerank=False)
+                e2 = rel_err(ids2, d2)
+                ent["traversal_max_rel_err"] = float(e2.max())
+                ent["traversal_mean_rel_err"] = float(e2.mean())
+                ent["recall@10_no_rerank"] = round(recall(torch, ids2, gt), 4)
+            res[name] = ent
+    for L in (64, 128):
+        f = res[f"f32@L{L}"]["recall@10"]
+        for s in ("bf16+rerank", "fp8+rerank"):
+            res[f"{s}@L{L}"]["recall_loss_vs_f32"] = round(f - res[f"{s}@L{L}"]["recall@10"], 4)
+    line = {"metric": "reduced precision on 5Mx96 float: recall@10, QPS and distance error vs FP64",
+            "config": {"workload": f"{n}x{D} float32, 2000 unit-norm centres, sigma 0.05; {nq} queries; "
+                                   f"R={R} L={L_BUILD} alpha={ALPHA}; k={K}", "build_s": round(build_s, 2)},
+            "data": "synthetic (seeded Gaussian mixture)", "forms": res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main_serve():
+    """Serving: a uint8 index (configuration 5: 10M x 128, 4,000 clusters, R=64) behind the
+    continuous-batching server; a Poisson stream of requests at --rate: searches of one
+    query with k in {1, 10, 100} and L uniform in 16..512, and write requests (insert or
+    delete batches, size log-uniform in 1..max-write).  Reports achieved throughput,
+    p50/p99 latency per kind, batching counters, and recall@10 of the k=10 searches."""
+    args = parse()
+    import threading as th
+
+    import torch
+
+    import vann
+    from vann import workload
+
+    dev = torch.device("cuda", 0)
+    n = args.n if args.n != N_BASE else 10_000_000
+    clusters = 4000 if n >= 1_000_000 else max(10, n // 2500)
+    base = workload.mixture(n, DIM, clusters, seed=1)
+    qpool = workload.mixture(20_000, DIM, clusters, seed=2)
+    base_d = torch.from_numpy(base).to(dev)
+    cap = int(n * 1.05)
+    idx = vann.Index(DIM, R, L_BUILD, ALPHA, capacity=cap, stores=("f32", "u8"))
+    t0 = time.time()
+    idx.build(base_d, batch=BATCH, seed=2024)
+    torch.cuda.synchronize()
+    build_s = time.time() - t0
+    del base_d
+    torch.cuda.empty_cache()
+    srv = vann.Server(idx, max_batch=4096, slots=4, max_k=100, store="u8",
+                      hbm_budget=4 * 4096 * (DIM * 4 + 100 * 8 + 8))
+    rng = np.random.default_rng(11)
+    nreq = int(args.rate * args.duration)
+    gaps = rng.exponential(1.0 / args.rate, nreq)
+    kinds = rng.random(nreq)
+    live = n
+    reqs = []
+    for i in range(nreq):
+        if kinds[i] >= args.write_frac:
+            k = int(rng.choice([1, 10, 100]))
+            L = max(k, int(rng.integers(16, 513)))
+            reqs.append(("search", int(rng.integers(0, len(qpool))), k, L))
+        else:
+            size = int(np.exp(rng.uniform(0, np.log(args.max_write))))
+            if rng.random() < 0.5:
+                reqs.append(("insert", size))
+            else:
+                reqs.append(("delete", rng.integers(0, n, size).astype(np.uint32)))
+    tickets, results = [None] * nreq, [None] * nreq
+
+    def waiter():
+        for i in range(nreq):
+            while tickets[i] is None:
+                time.sleep(0.0002)
+            results[i] = srv.wait(tickets[i])
+
+    w = th.Thread(target=waiter)
+    w.start()
+    ins_seed = 5000
+    t_start = time.perf_counter()
+    t_next = t_start
+    for i, rq in enumerate(reqs):
+        t_next += gaps[i]
+        while time.perf_counter() < t_next:
+            pass
+        if rq[0] == "search":
+            tickets[i] = srv.submit_search(qpool[rq[1]], rq[2], rq[3])
+        elif rq[0] == "insert":
+            ins_seed += 1
+            tickets[i] = srv.submit_insert(workload.mixture(rq[1], DIM, clusters, seed=ins_seed))
+        else:
+            tickets[i] = srv.submit_delete(rq[1])
+    t_submitted = time.perf_counter()
+    w.join()
+    t_end = time.perf_counter()
+    stats = srv.stats()
+    srv.close()
+    lat = {"search": [], "insert": [], "delete": []}
+    for rq, res in zip(reqs, results):
+        lat[rq[0]].append(res[2])
+    # recall@10 of the k=10 searches against FP64 brute force on the original rows
+    sel = [(i, rq) for i, rq in enumerate(reqs) if rq[0] == "search" and rq[2] == 10][:2000]
+    rec = None
+    if sel:
+        qs = torch.from_numpy(qpool[[rq[1] for _, rq in sel]]).to(dev)
+        gt = ground_truth(torch, torch.from_numpy(base).to(dev), qs, K)
+        got = torch.from_numpy(np.stack([results[i][0][0, :10].astype(np.int64) for i, _ in sel])).to(dev)
+        rec = recall(torch, got.int(), gt)
+
+    def pct(v, p):
+        return round(float(np.percentile(v, p)) / 1e3, 3) if v else None
+
+    line = {"metric": "serving: p50/p99 latency and throughput under a Poisson request stream",
+            "config": {"workload": f"{n}x{DIM} uint8-valued, {clusters}-cluster mixture; R={R} L={L_BUILD}; "
+                                   f"offered {args.rate:.0f} req/s for {args.duration} s; "
+                                   f"{100 * (1 - args.write_frac):.0f}% searches k in {{1,10,100}}, "
+                                   f"L in 16..512; writes log-uniform 1..{args.max_write}",
+                       "build_s": round(build_s, 2), "store": "u8"},
+            "offered_req_per_s": args.rate, "requests": nreq,
+            "achieved_req_per_s": round(nreq / (t_end - t_start), 1),
+            "submit_lag_s": round(t_submitted - t_start - float(gaps.sum()), 3),
+            "search_p50_ms": pct(lat["search"], 50), "search_p99_ms": pct(lat["search"], 99),
+            "insert_p50_ms": pct(lat["insert"], 50), "insert_p99_ms": pct(lat["insert"], 99),
+            "delete_p50_ms": pct(lat["delete"], 50), "delete_p99_ms": pct(lat["delete"], 99),
+            "recall@10_k10_searches": rec, "server": stats}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 if __name__ == "__main__":
     if "--impl" in sys.argv and sys.argv[sys.argv.index("--impl") + 1] == "reference":
         sys.exit(main_reference())
+    if "--config" in sys.argv:
+        cfg = sys.argv[sys.argv.index("--config") + 1]
+        if cfg == "churn":
+            sys.exit(main_churn())
+        if cfg == "precision":
+            sys.exit(main_precision())
+        if cfg == "serve":
+            sys.exit(main_serve())
     sys.exit(main())

@@ -97,6 +97,40 @@ cudaError_t launch_convert(const float* src, void* dst, float* scale, uint64_t r
     return cudaGetLastError();
 }
 
+// Same conversion for rows scattered over an id list (inserts into reused ids):
+// one warp per listed row, the row's traversal copy rewritten from its FP32 row.
+__global__ void convert_ids_kernel(const float* vecs, const uint32_t* ids, uint64_t n, void* dst,
+                                   float* scale, uint32_t D, int store) {
+    uint64_t i    = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
+    uint32_t lane = threadIdx.x & 31u;
+    if (i >= n) return;
+    const uint64_t r = ids[i];
+    const float*   s = vecs + r * D;
+    if (store == 1) {
+        __nv_bfloat16* d = static_cast<__nv_bfloat16*>(dst) + r * D;
+        for (uint32_t k = lane; k < D; k += 32) d[k] = __float2bfloat16_rn(s[k]);
+    } else if (store == 2) {
+        float amax = 0.f;
+        for (uint32_t k = lane; k < D; k += 32) amax = fmaxf(amax, fabsf(s[k]));
+        for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+        float    sc  = amax > 0.f ? amax / 448.f : 1.f;
+        float    inv = 1.f / sc;
+        uint8_t* d   = static_cast<uint8_t*>(dst) + r * D;
+        for (uint32_t k = lane; k < D; k += 32)
+            d[k] = (uint8_t)__nv_cvt_float_to_fp8(s[k] * inv, __NV_SATFINITE, __NV_E4M3);
+        if (lane == 0) scale[r] = sc;
+    } else if (store == 3) {
+        uint8_t* d = static_cast<uint8_t*>(dst) + r * D;
+        for (uint32_t k = lane; k < D; k += 32) d[k] = (uint8_t)fminf(fmaxf(rintf(s[k]), 0.f), 255.f);
+    }
+}
+cudaError_t launch_convert_ids(const float* vecs, const uint32_t* ids, uint64_t n, void* dst, float* scale,
+                               uint32_t D, int store, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    convert_ids_kernel<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(vecs, ids, n, dst, scale, D, store);
+    return cudaGetLastError();
+}
+
 __global__ void iota_kernel(uint32_t* out, uint64_t n, uint32_t first) {
     uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (i < n) out[i] = first + (uint32_t)i;

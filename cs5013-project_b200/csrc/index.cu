@@ -127,6 +127,9 @@ struct vann_index {
     size_t    held     = 0;
 
     std::vector<uint32_t> free_ids;  // consolidated ids, reused by inserts
+    // per-query L / k arrays of the vann_search_uneven call in progress
+    const uint32_t* pending_Lq = nullptr;
+    const uint32_t* pending_kq = nullptr;
     // autotuned search variant per (store, rerank, L)
     std::map<std::tuple<uint32_t, uint32_t, uint32_t>, int> tuned;
 
@@ -357,6 +360,10 @@ vann_status vann_create(const vann_params* params, vann_index** out) {
         VREQUIRE(p.max_reverse >= 1 && p.max_reverse <= 2048, VANN_ERR_INVALID,
                  "max_reverse must be in [1, 2048]");
         VREQUIRE(p.alpha >= 1.0f, VANN_ERR_INVALID, "alpha must be >= 1");
+        VREQUIRE(!(p.stores & (1u << VANN_STORE_BF16)) || p.dim % 8 == 0, VANN_ERR_UNSUPPORTED,
+                 "the bf16 copy needs dim to be a multiple of 8");
+        VREQUIRE(!(p.stores & ((1u << VANN_STORE_FP8) | (1u << VANN_STORE_U8))) || p.dim % 16 == 0,
+                 VANN_ERR_UNSUPPORTED, "one-byte copies need dim to be a multiple of 16");
         auto* h = new vann_index();
         try {
             h->p = p;
@@ -592,6 +599,8 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
         a.hops_out = d_hops;
         a.evals_out = d_evals;
         a.adjw_out = d_adjw;
+        a.Lq = h->pending_Lq;
+        a.kq = h->pending_kq;
         a.counter = h->next_counter(S(stream));
         a.status = h->status;
         VCHECK(vann::launch_search(a, (int)sp->store, h->num_sms, S(stream), h->variant_for(*sp)));
@@ -644,6 +653,17 @@ vann_status vann_search(vann_index* h, const float* d_queries, uint64_t nq,
     return vann_search_stats(h, d_queries, nq, sp, d_ids, d_dists, nullptr, nullptr, nullptr, stream);
 }
 
+vann_status vann_search_uneven(vann_index* h, const float* d_queries, uint64_t nq, const vann_search_params* sp,
+                               const uint32_t* d_L, const uint32_t* d_k, uint32_t* d_ids, float* d_dists,
+                               void* stream) {
+    h->pending_Lq = d_L;
+    h->pending_kq = d_k;
+    vann_status s = vann_search_stats(h, d_queries, nq, sp, d_ids, d_dists, nullptr, nullptr, nullptr, stream);
+    h->pending_Lq = nullptr;
+    h->pending_kq = nullptr;
+    return s;
+}
+
 vann_status vann_sync(vann_index* h, void* stream) {
     vann_status result = VANN_OK;
     vann_status s = guard([&] {
@@ -684,8 +704,10 @@ vann_status vann_insert(vann_index* h, const float* d_vecs, uint64_t n, uint32_t
         if (reuse == 0) {
             h->convert_rows(h->size, n, st);
         } else {
-            // reused ids are scattered: convert every touched row one by one
-            for (uint64_t i = 0; i < n; ++i) h->convert_rows(ids[i], 1, st);
+            for (int s = 1; s < 4; ++s)  // reused ids are scattered: convert by id list
+                if (h->store[s])
+                    VCHECK(vann::launch_convert_ids(h->vecs, h->nodes.as<uint32_t>(), n, h->store[s],
+                                                    s == 2 ? h->fp8_scale : nullptr, D, s, st));
         }
         h->size += n - reuse;
         const bool parity = (h->p.flags & VANN_QUIRK_SKIP_BATCH_INDEX) != 0;

@@ -23,7 +23,9 @@ struct SearchArgs {
     const float*    queries;   // nq x D FP32
     uint64_t        nq;
     uint32_t        D;
-    uint32_t        L, k, entry, max_hops;
+    uint32_t        L, k, entry, max_hops;   // L, k: the launch's maxima
+    const uint32_t* Lq;        // per-query worklist size (<= L) or null
+    const uint32_t* kq;        // per-query result count (<= k) or null
     uint32_t        skip_mode;  // 0 none, 1 batch index, 2 skip_base + batch index
     uint32_t        skip_base;
     int             rerank;
@@ -84,6 +86,8 @@ cudaError_t launch_hash_rows(const uint32_t* adj, uint32_t* adj_h, uint64_t n, u
                              cudaStream_t st);
 cudaError_t launch_convert(const float* src, void* dst, float* scale, uint64_t rows, uint32_t D,
                            int store, cudaStream_t st);
+cudaError_t launch_convert_ids(const float* vecs, const uint32_t* ids, uint64_t n, void* dst, float* scale,
+                               uint32_t D, int store, cudaStream_t st);
 cudaError_t launch_iota(uint32_t* out, uint64_t n, uint32_t first, cudaStream_t st);
 cudaError_t launch_set_bits(uint32_t* bits, const uint32_t* ids, uint64_t n, uint64_t limit,
                             cudaStream_t st);

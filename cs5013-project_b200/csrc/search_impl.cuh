@@ -77,7 +77,6 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
     float*           nb_d  = reinterpret_cast<float*>(base + 5008 + 8 * lay.lp + 4 * lay.maxr);
     uint64_t*        nb_key = reinterpret_cast<uint64_t*>(nb_id);  // same bytes, after the ids/dists are read
     uint64_t*        keys  = reinterpret_cast<uint64_t*>(base + 5008 + 8 * lay.lp + 8 * lay.maxr);
-    const uint32_t   L     = a.L;
     const uint32_t   R     = a.R;
 
     for (;;) {
@@ -85,6 +84,10 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
         if (lane == 0) q = atomicAdd(a.counter, 1u);
         q = __shfl_sync(0xffffffffu, q, 0);
         if (q >= a.nq) break;
+        // per-query worklist size and result count (uneven batches), capped by the
+        // launch's maximum, which sized the shared memory and the output rows
+        const uint32_t L  = a.Lq != nullptr ? max(1u, min(__ldg(a.Lq + q), a.L)) : a.L;
+        const uint32_t kq = a.kq != nullptr ? min(__ldg(a.kq + q), a.k) : a.k;
 
         Query<S, DC> qv;
         load_query<S, DC>(qv, a.queries + (uint64_t)q * a.D, a.D, lane);
@@ -334,7 +337,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
                 warp_bitonic_sort_smem(keys, lay.keys, lane);
                 for (uint32_t t = lane; t < a.k; t += 32) {
                     uint64_t o = (uint64_t)q * a.k + t;
-                    if (t < n) {
+                    if (t < n && t < kq) {
                         a.out_ids[o] = wl_id[(uint32_t)keys[t]] & ~kVisitedBit;
                         a.out_d[o]   = key_dist(keys[t]);
                     } else {
@@ -345,7 +348,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
             } else {
                 for (uint32_t t = lane; t < a.k; t += 32) {
                     uint64_t o = (uint64_t)q * a.k + t;
-                    if (t < n) {
+                    if (t < n && t < kq) {
                         a.out_ids[o] = wl_id[t] & ~kVisitedBit;
                         a.out_d[o]   = wl_d[t];
                     } else {

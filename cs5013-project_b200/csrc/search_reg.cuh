@@ -83,7 +83,6 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
     float*          nb_d  = reinterpret_cast<float*>(base + 5008 + 4 * lay.maxr);
     uint64_t*       nb_key = reinterpret_cast<uint64_t*>(nb_id);  // after ids/dists are read
     uint64_t*       rkeys = reinterpret_cast<uint64_t*>(base);     // rerank keys, after the search
-    const uint32_t  L     = a.L;
     const uint32_t  R     = a.R;
 
     for (;;) {
@@ -91,6 +90,10 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
         if (lane == 0) q = atomicAdd(a.counter, 1u);
         q = __shfl_sync(0xffffffffu, q, 0);
         if (q >= a.nq) break;
+        // per-query worklist size and result count (uneven batches), capped by the
+        // launch's maximum, which sized the shared memory and the output rows
+        const uint32_t L  = a.Lq != nullptr ? max(1u, min(__ldg(a.Lq + q), a.L)) : a.L;
+        const uint32_t kq = a.kq != nullptr ? min(__ldg(a.kq + q), a.k) : a.k;
 
         Query<S, DC> qv;
         load_query<S, DC>(qv, a.queries + (uint64_t)q * a.D, a.D, lane);
@@ -321,7 +324,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
                 warp_bitonic_sort_smem(rkeys, ns, lane);
                 for (uint32_t t = lane; t < a.k; t += 32) {
                     uint64_t o = (uint64_t)q * a.k + t;
-                    if (t < n) {
+                    if (t < n && t < kq) {
                         a.out_ids[o] = nb_id[(uint32_t)rkeys[t]];
                         a.out_d[o]   = key_dist(rkeys[t]);
                     } else {
@@ -335,8 +338,8 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
                     uint32_t e = (uint32_t)r * 32u + lane;
                     if (e < a.k) {
                         uint64_t o   = (uint64_t)q * a.k + e;
-                        a.out_ids[o] = e < n ? (wp[r] & ~kVisitedBit) : kNone;
-                        a.out_d[o]   = e < n ? key_dist(wk[r]) : __int_as_float(0x7f800000);
+                        a.out_ids[o] = e < n && e < kq ? (wp[r] & ~kVisitedBit) : kNone;
+                        a.out_d[o]   = e < n && e < kq ? key_dist(wk[r]) : __int_as_float(0x7f800000);
                     }
                 }
             }

@@ -30,8 +30,10 @@ NONE_ID = 0xFFFFFFFF
 EXPORTS = [
     "vann_status_string", "vann_last_error", "vann_abi_version", "vann_create", "vann_destroy",
     "vann_get_info", "vann_load_graph", "vann_save_graph", "vann_set_graph", "vann_get_graph",
-    "vann_build", "vann_build_loaded", "vann_search", "vann_search_stats", "vann_autotune", "vann_search_variant_count", "vann_sync", "vann_insert", "vann_delete", "vann_delete_by_vector",
-    "vann_consolidate", "vann_medoid_noalloc",
+    "vann_build", "vann_build_loaded", "vann_search", "vann_search_stats", "vann_search_uneven", "vann_autotune", "vann_search_variant_count", "vann_sync", "vann_insert", "vann_delete", "vann_delete_by_vector",
+    "vann_consolidate", "vann_medoid_noalloc", "vann_server_create", "vann_server_destroy",
+    "vann_server_submit_search", "vann_server_submit_insert", "vann_server_submit_delete",
+    "vann_server_submit_consolidate", "vann_server_wait", "vann_server_get_stats",
 ]
 
 
@@ -56,6 +58,17 @@ class Info(C.Structure):
     _fields_ = [("size", C.c_uint64), ("capacity", C.c_uint64), ("live", C.c_uint64),
                 ("free_ids", C.c_uint64), ("entry", C.c_uint32), ("dim", C.c_uint32),
                 ("degree", C.c_uint32), ("consistent", C.c_uint32), ("device_bytes", C.c_uint64)]
+
+
+class ServerParams(C.Structure):
+    _fields_ = [("max_batch", C.c_uint32), ("slots", C.c_uint32), ("hbm_budget", C.c_uint64),
+                ("max_k", C.c_uint32), ("store", C.c_uint32), ("rerank", C.c_uint32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("slot_bytes", C.c_uint64), ("batches", C.c_uint64),
+                ("queries", C.c_uint64), ("writes", C.c_uint64), ("max_inflight", C.c_uint64),
+                ("queued", C.c_uint64)]
 
 
 _lib = None
@@ -84,6 +97,7 @@ def lib():
             "vann_build_loaded": (C.c_int, [vp, vp]),
             "vann_search": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp, vp]),
             "vann_search_stats": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp, vp, vp, vp, vp]),
+            "vann_search_uneven": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp, vp, vp, vp]),
             "vann_autotune": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp]),
             "vann_search_variant_count": (C.c_int, []),
             "vann_sync": (C.c_int, [vp, vp]),
@@ -92,6 +106,14 @@ def lib():
             "vann_delete_by_vector": (C.c_int, [vp, vp, u64, vp, vp]),
             "vann_consolidate": (C.c_int, [vp, vp]),
             "vann_medoid_noalloc": (C.c_int, [vp, u64, u32, vp, vp]),
+            "vann_server_create": (C.c_int, [vp, C.POINTER(ServerParams), C.POINTER(vp)]),
+            "vann_server_destroy": (C.c_int, [vp]),
+            "vann_server_submit_search": (C.c_int, [vp, vp, u32, u32, u32, C.POINTER(u64)]),
+            "vann_server_submit_insert": (C.c_int, [vp, vp, u32, C.POINTER(u64)]),
+            "vann_server_submit_delete": (C.c_int, [vp, vp, u32, C.POINTER(u64)]),
+            "vann_server_submit_consolidate": (C.c_int, [vp, C.POINTER(u64)]),
+            "vann_server_wait": (C.c_int, [vp, u64, vp, vp, C.POINTER(C.c_double), u32]),
+            "vann_server_get_stats": (C.c_int, [vp, C.POINTER(ServerStats)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -205,6 +227,21 @@ class Index:
                                  _dev(ids, torch.int32), _dev(dists, torch.float32), _stream_ptr(stream)))
         return ids, dists
 
+    def search_uneven(self, queries, L, k, store: str = "f32", rerank: bool = False, quirks: int = 0,
+                      stream=None):
+        """One launch over queries with their own L[i] and k[i] (int32 CUDA tensors);
+        returns (ids, dists) with max(k) columns, padded past k[i]."""
+        torch = _torch()
+        nq = queries.shape[0]
+        Lmax, kmax = int(L.max().item()), int(k.max().item())
+        ids = torch.empty((nq, kmax), dtype=torch.int32, device=queries.device)
+        dists = torch.empty((nq, kmax), dtype=torch.float32, device=queries.device)
+        sp = SearchParams(Lmax, kmax, STORES[store], int(rerank), quirks, 0)
+        _check(lib().vann_search_uneven(self._h, _dev(queries, torch.float32), nq, C.byref(sp),
+                                        _dev(L, torch.int32), _dev(k, torch.int32), _dev(ids, torch.int32),
+                                        _dev(dists, torch.float32), _stream_ptr(stream)))
+        return ids, dists
+
     def search_stats(self, queries, k: int, L: int, store: str = "f32", rerank: bool = False,
                      quirks: int = 0, max_hops: int = 0, stream=None):
         """search() plus per-query (hops, distance evaluations, adjacency words)."""
@@ -256,6 +293,76 @@ class Index:
 
     def consolidate(self, stream=None):
         _check(lib().vann_consolidate(self._h, _stream_ptr(stream)))
+
+
+class Server:
+    """Continuous-batching request loop over one Index (vann_server_*).  Requests
+    carry host (numpy) data; submit_* return tickets, wait() returns results."""
+
+    def __init__(self, index: "Index", max_batch: int = 4096, slots: int = 4, hbm_budget: int = 0,
+                 max_k: int = 100, store: str = "f32", rerank: bool = False):
+        p = ServerParams(max_batch, slots, hbm_budget, max_k, STORES[store], int(rerank))
+        h = C.c_void_p()
+        _check(lib().vann_server_create(index._h, C.byref(p), C.byref(h)))
+        self._h, self.index, self.dim = h, index, index.dim
+        self._kind = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().vann_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit_search(self, q, k: int, L: int) -> int:
+        import numpy as np
+        q = np.ascontiguousarray(q, dtype=np.float32).reshape(-1, self.dim)
+        t = C.c_uint64()
+        _check(lib().vann_server_submit_search(self._h, q.ctypes.data, q.shape[0], k, L, C.byref(t)))
+        self._kind[t.value] = ("search", q.shape[0], k)
+        return t.value
+
+    def submit_insert(self, vecs) -> int:
+        import numpy as np
+        v = np.ascontiguousarray(vecs, dtype=np.float32).reshape(-1, self.dim)
+        t = C.c_uint64()
+        _check(lib().vann_server_submit_insert(self._h, v.ctypes.data, v.shape[0], C.byref(t)))
+        self._kind[t.value] = ("insert", v.shape[0], 1)
+        return t.value
+
+    def submit_delete(self, ids) -> int:
+        import numpy as np
+        i = np.ascontiguousarray(ids, dtype=np.uint32)
+        t = C.c_uint64()
+        _check(lib().vann_server_submit_delete(self._h, i.ctypes.data, i.shape[0], C.byref(t)))
+        self._kind[t.value] = ("delete", i.shape[0], 0)
+        return t.value
+
+    def submit_consolidate(self) -> int:
+        t = C.c_uint64()
+        _check(lib().vann_server_submit_consolidate(self._h, C.byref(t)))
+        self._kind[t.value] = ("consolidate", 0, 0)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 0):
+        """-> (ids, dists, latency_us); ids/dists are n x k for searches, the new ids for inserts."""
+        import numpy as np
+        kind, n, k = self._kind.pop(ticket)
+        ids = np.empty((n, k), np.uint32) if kind == "search" else np.empty(n, np.uint32)
+        d = np.empty((n, k), np.float32) if kind == "search" else None
+        lat = C.c_double()
+        _check(lib().vann_server_wait(self._h, ticket, ids.ctypes.data if n else None,
+                                      d.ctypes.data if d is not None else None, C.byref(lat), timeout_ms))
+        return ids, d, lat.value
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        _check(lib().vann_server_get_stats(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in ServerStats._fields_}
 
 
 def medoid_noalloc(vecs, out, stream=None):

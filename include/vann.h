@@ -145,6 +145,14 @@ vann_status vann_autotune(vann_index* index, const float* d_queries, uint64_t nq
 /* Number of compiled search variants (length of vann_autotune's h_ms_out,
  * which may be NULL; it receives the mean ms of each variant). */
 int vann_search_variant_count(void);
+/* vann_search over a batch whose queries have their own worklist size and result
+ * count: d_L[i] <= sp->L and d_k[i] <= sp->k (device arrays of nq; sp->L, sp->k
+ * are the batch maxima and size the launch).  Row i of d_ids / d_dists has
+ * stride sp->k and is padded past d_k[i] with UINT32_MAX / +inf.  One launch
+ * serves the whole uneven batch.  Asynchronous on `stream`. */
+vann_status vann_search_uneven(vann_index* index, const float* d_queries, uint64_t nq,
+                               const vann_search_params* sp, const uint32_t* d_L, const uint32_t* d_k,
+                               uint32_t* d_ids, float* d_dists, void* stream);
 /* Device status word of earlier asynchronous calls: synchronises `stream`,
  * returns VANN_ERR_HOP_LIMIT if a search hit its hop cap since the last call,
  * and clears it. */
@@ -170,6 +178,46 @@ vann_status vann_delete_by_vector(vann_index* index, const float* d_vecs, uint64
  * re-pruned over its live out-neighbours plus the deleted nodes' live
  * out-neighbours; deleted ids are then freed for reuse.  Synchronises. */
 vann_status vann_consolidate(vann_index* index, void* stream);
+
+/* ---------------------------------------------------------------- serving loop
+ * No counterpart in the reference, whose driver issues one call at a time on the
+ * default stream (vamana.cu:1782-1895).  A server owns a worker thread over one
+ * index.  Requests carry host data.  Searches queued while batch slots are busy
+ * are admitted together into the next free slot as one uneven launch (own k
+ * and L per request) with its copies on the slot's stream, so several batches
+ * run at once (continuous batching).  Writes keep their place in the request
+ * order: each search sees exactly the writes submitted before it.  Slot device
+ * memory is allocated at creation and capped by hbm_budget. */
+typedef struct {
+    uint32_t max_batch;   /* queries per admitted batch */
+    uint32_t slots;       /* batches on the GPU at once (one stream each) */
+    uint64_t hbm_budget;  /* device bytes for batch slots (0 = no cap); fewer slots if smaller */
+    uint32_t max_k;       /* largest k a search may ask for */
+    uint32_t store;       /* vann_store searches traverse */
+    uint32_t rerank;      /* exact FP32 rerank */
+} vann_server_params;
+
+typedef struct {
+    uint32_t slots;        /* slots admitted under the budget */
+    uint64_t slot_bytes;   /* device bytes per slot */
+    uint64_t batches, queries, writes, max_inflight, queued;
+} vann_server_stats;
+
+typedef struct vann_server vann_server;
+
+vann_status vann_server_create(vann_index* index, const vann_server_params* params, vann_server** out);
+vann_status vann_server_destroy(vann_server* server);
+/* n <= max_batch host queries (n x dim FP32), k <= max_k, k <= L <= 1024. */
+vann_status vann_server_submit_search(vann_server* server, const float* h_queries, uint32_t n, uint32_t k,
+                                      uint32_t L, uint64_t* ticket);
+vann_status vann_server_submit_insert(vann_server* server, const float* h_vecs, uint32_t n, uint64_t* ticket);
+vann_status vann_server_submit_delete(vann_server* server, const uint32_t* h_ids, uint32_t n, uint64_t* ticket);
+vann_status vann_server_submit_consolidate(vann_server* server, uint64_t* ticket);
+/* Blocks until the request is done (timeout_ms 0 = 10 minutes).  Search: n x k ids
+ * and distances; insert: the n new ids in h_ids.  latency_us: submit to done. */
+vann_status vann_server_wait(vann_server* server, uint64_t ticket, uint32_t* h_ids, float* h_dists,
+                             double* latency_us, uint32_t timeout_ms);
+vann_status vann_server_get_stats(vann_server* server, vann_server_stats* out);
 
 /* Allocation-free entry-point selection.  No counterpart in the reference.
  * Computes the medoid used as the search entry point (argmin over the n rows

@@ -154,3 +154,24 @@ def test_autotuned_variant_is_still_exact(oracle, vann_mod, graph64):
         ids, d = idx.search(qd, k=10, L=48, store=store)
         assert np.array_equal(ids.cpu().numpy().view(np.uint32), oids)
         assert np.array_equal(d.cpu().numpy(), od)
+
+
+def test_uneven_batch_equals_separate_launches(oracle, vann_mod, graph64):
+    """One launch with its own (k, L) per query gives, query by query, exactly the
+    results of a separate search with that k and L (the rest of the row padded)."""
+    import torch
+
+    base, g, entry = graph64
+    q = workload.mixture(96, 128, 40, seed=93)
+    idx = _gpu_index(vann_mod, base, g, entry)
+    rng = np.random.default_rng(1)
+    ks = rng.choice([1, 10, 50], 96).astype(np.int32)
+    Ls = np.maximum(ks, rng.integers(16, 200, 96)).astype(np.int32)
+    qd = torch.from_numpy(q).cuda()
+    ids, d = idx.search_uneven(qd, torch.from_numpy(Ls).cuda(), torch.from_numpy(ks).cuda())
+    ids, d = ids.cpu().numpy().view(np.uint32), d.cpu().numpy()
+    for i in range(96):
+        a, b = idx.search(qd[i:i + 1].contiguous(), k=int(ks[i]), L=int(Ls[i]))
+        assert np.array_equal(ids[i, :ks[i]], a.cpu().numpy().view(np.uint32)[0])
+        assert np.array_equal(d[i, :ks[i]], b.cpu().numpy()[0])
+        assert (ids[i, ks[i]:] == 0xFFFFFFFF).all()

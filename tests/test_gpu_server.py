@@ -1,0 +1,85 @@
+"""The continuous-batching server: every result of a mixed burst of requests (uneven k
+and L, inserts, deletes, consolidation) equals the same request run alone, one call at a
+time, on an identically built index.  Search ids and distances are compared bit for bit."""
+import numpy as np
+import pytest
+
+from vann import workload
+
+pytestmark = pytest.mark.gpu
+
+
+def _index(vann_mod, base):
+    import torch
+
+    idx = vann_mod.Index(128, 32, 64, 1.2, capacity=len(base) + 2000)
+    idx.build(torch.from_numpy(base).cuda(), batch=0, seed=13)
+    return idx
+
+
+def test_server_mixed_results_equal_alone(vann_mod):
+    import torch
+
+    base = workload.mixture(8000, 128, 30, seed=81)
+    served, alone = _index(vann_mod, base), _index(vann_mod, base)
+    srv = vann_mod.Server(served, max_batch=256, slots=4, max_k=100)
+    rng = np.random.default_rng(5)
+    ops, live_initial = [], list(range(len(base)))
+    for i in range(400):
+        u = rng.random()
+        if u < 0.9:
+            nqr = int(rng.integers(1, 5))
+            k = int(rng.choice([1, 10, 100]))
+            L = max(k, int(rng.integers(16, 257)))
+            ops.append(("search", workload.mixture(nqr, 128, 30, seed=10_000 + i), k, L))
+        elif u < 0.95:
+            ops.append(("insert", workload.mixture(int(rng.integers(1, 40)), 128, 30, seed=20_000 + i)))
+        elif u < 0.99:
+            pick = rng.choice(len(live_initial), int(rng.integers(1, 20)), replace=False)
+            ids = np.array([live_initial[j] for j in pick], np.uint32)
+            live_initial = [x for j, x in enumerate(live_initial) if j not in set(pick.tolist())]
+            ops.append(("delete", ids))
+        else:
+            ops.append(("consolidate",))
+    # the whole burst is queued at once, so searches share batches
+    tickets = []
+    for op in ops:
+        if op[0] == "search":
+            tickets.append(srv.submit_search(op[1], op[2], op[3]))
+        elif op[0] == "insert":
+            tickets.append(srv.submit_insert(op[1]))
+        elif op[0] == "delete":
+            tickets.append(srv.submit_delete(op[1]))
+        else:
+            tickets.append(srv.submit_consolidate())
+    results = [srv.wait(t) for t in tickets]
+    st = srv.stats()
+    n_search = sum(op[0] == "search" for op in ops)
+    print(st, n_search)
+    assert st["batches"] < n_search  # requests were batched together
+    srv.close()
+
+    for op, (ids, d, lat) in zip(ops, results):
+        assert lat > 0
+        if op[0] == "search":
+            gi, gd = alone.search(torch.from_numpy(op[1]).cuda(), k=op[2], L=op[3])
+            assert np.array_equal(ids, gi.cpu().numpy().view(np.uint32))
+            assert np.array_equal(d, gd.cpu().numpy())
+        elif op[0] == "insert":
+            new = alone.insert(torch.from_numpy(op[1]).cuda()).cpu().numpy().view(np.uint32)
+            assert np.array_equal(ids, new)
+        elif op[0] == "delete":
+            alone.delete(torch.from_numpy(op[1].astype(np.int32)).cuda())
+        else:
+            alone.consolidate()
+
+
+def test_server_budget_caps_slots(vann_mod):
+    base = workload.mixture(2000, 128, 10, seed=82)
+    idx = _index(vann_mod, base)
+    slot = 64 * (128 * 4 + 10 * 8 + 8)
+    srv = vann_mod.Server(idx, max_batch=64, slots=8, max_k=10, hbm_budget=3 * slot)
+    assert srv.stats()["slots"] == 3
+    srv.close()
+    with pytest.raises(vann_mod.VannError):
+        vann_mod.Server(idx, max_batch=64, slots=8, max_k=10, hbm_budget=slot - 1)
