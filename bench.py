@@ -562,7 +562,7 @@ def main_precision():
     from vann import workload
 
     dev = torch.device("cuda", 0)
-    n = args.n if args.n != N_BASE else 5_000_000
+    n = args.n if "--n" in sys.argv else 5_000_000  # configuration 4 is 5M rows
     nq, D = args.nq, 96
     base = workload.mixture(n, D, 2000, seed=11, sigma=0.05, integer=False, unit_norm=True)
     q = workload.mixture(nq, D, 2000, seed=12, sigma=0.05, integer=False, unit_norm=True)
@@ -627,7 +627,7 @@ def main_serve():
     from vann import workload
 
     dev = torch.device("cuda", 0)
-    n = args.n if args.n != N_BASE else 10_000_000
+    n = args.n if "--n" in sys.argv else 10_000_000  # configuration 5 is 10M rows
     clusters = 4000 if n >= 1_000_000 else max(10, n // 2500)
     base = workload.mixture(n, DIM, clusters, seed=1)
     qpool = workload.mixture(20_000, DIM, clusters, seed=2)

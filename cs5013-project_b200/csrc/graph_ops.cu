@@ -208,7 +208,7 @@ __global__ void edges_kernel(const uint32_t* nodes, uint64_t n_nodes, const uint
         uint32_t tg = adj[(uint64_t)node * R + j];
         keys[t]     = tg;
         vals[t]     = node;
-        atomicAdd(counts + tg, 1u);
+        if (counts != nullptr) atomicAdd(counts + tg, 1u);
     } else {
         keys[t] = kNone;
         vals[t] = kNone;

@@ -138,7 +138,7 @@ struct vann_index {
         return it == tuned.end() ? 0 : it->second;
     }
 
-    DevBuf vis_ids, vis_d, vis_n, nodes, e_keys, e_vals, e_keys2, e_vals2, counts, offsets, cub_tmp,
+    DevBuf vis_ids, vis_d, vis_n, nodes, runs, e_keys, e_vals, e_keys2, e_vals2, counts, offsets, cub_tmp,
         medoid_ws, gather, cand, cand_n, cand_d, list_n, out_tmp;
 
     void alloc(void** ptr, size_t bytes) {
@@ -155,7 +155,7 @@ struct vann_index {
         cudaFree(tomb);
         cudaFree(counters);
         cudaFree(status);
-        for (DevBuf* b : {&vis_ids, &vis_d, &vis_n, &nodes, &e_keys, &e_vals, &e_keys2, &e_vals2,
+        for (DevBuf* b : {&vis_ids, &vis_d, &vis_n, &nodes, &runs, &e_keys, &e_vals, &e_keys2, &e_vals2,
                           &counts, &offsets, &cub_tmp, &medoid_ws, &gather, &cand, &cand_n, &cand_d,
                           &list_n, &out_tmp})
             b->release();
@@ -250,34 +250,13 @@ struct vann_index {
         VCHECK(vann::launch_prune(pa, num_sms, st));
 
         // reverse edges, sorted by target with sources in batch order (stable)
-        const uint64_t ne = count * R;
+        const uint64_t ne             = count * R;
+        const bool     consistent_rev = consistent || all_nodes;
         e_keys.ensure(sizeof(uint32_t) * ne);
         e_vals.ensure(sizeof(uint32_t) * ne);
         e_keys2.ensure(sizeof(uint32_t) * ne);
         e_vals2.ensure(sizeof(uint32_t) * ne);
-        // sized by capacity once, so no buffer is freed while earlier batches run
-        counts.ensure(sizeof(uint32_t) * (p.capacity + 1));
-        offsets.ensure(sizeof(uint32_t) * (p.capacity + 1));
-        VCHECK(cudaMemsetAsync(counts.p, 0, sizeof(uint32_t) * (size + 1), st));
-        VCHECK(vann::launch_edges(d_nodes, count, deg, adj, R, e_keys.as<uint32_t>(),
-                                  e_vals.as<uint32_t>(), counts.as<uint32_t>(), st));
         const int end_bit = 32;  // padded slots carry UINT32_MAX keys
-        size_t tmp_sort = 0, tmp_scan = 0;
-        VCHECK(cub::DeviceRadixSort::SortPairs(nullptr, tmp_sort, e_keys.as<uint32_t>(),
-                                               e_keys2.as<uint32_t>(), e_vals.as<uint32_t>(),
-                                               e_vals2.as<uint32_t>(), (int)ne, 0, end_bit, st));
-        VCHECK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_scan, counts.as<uint32_t>(),
-                                             offsets.as<uint32_t>(), (int)(size + 1), st));
-        cub_tmp.ensure(std::max(tmp_sort, tmp_scan));
-        size_t t1 = cub_tmp.bytes;
-        VCHECK(cub::DeviceRadixSort::SortPairs(cub_tmp.p, t1, e_keys.as<uint32_t>(),
-                                               e_keys2.as<uint32_t>(), e_vals.as<uint32_t>(),
-                                               e_vals2.as<uint32_t>(), (int)ne, 0, end_bit, st));
-        size_t t2 = cub_tmp.bytes;
-        VCHECK(cub::DeviceScan::ExclusiveSum(cub_tmp.p, t2, counts.as<uint32_t>(),
-                                             offsets.as<uint32_t>(), (int)(size + 1), st));
-
-        const bool consistent_rev = consistent || all_nodes;
         vann::PruneArgs ra{};
         ra.vecs = vecs;
         ra.D = p.dim;
@@ -287,16 +266,74 @@ struct vann_index {
         ra.R = R;
         ra.alpha = p.alpha;
         ra.cap = p.max_reverse;
-        ra.node_ids = nullptr;
-        ra.n_nodes = size;
-        ra.csr_off = offsets.as<uint32_t>();
-        ra.csr_cnt = counts.as<uint32_t>();
         ra.csr_src = e_vals2.as<uint32_t>();
         ra.use_b = 1;
-        ra.skip_empty = consistent_rev ? 1 : 0;
-        ra.consistent = consistent_rev ? 1 : 0;
-        ra.counter = next_counter(st);
         ra.status = status;
+        if (consistent_rev) {
+            // Only the targets of new edges change: their ids and source runs come
+            // from a run-length encoding of the sorted edge list, so this pass costs
+            // O(batch * R), not O(index size).
+            runs.ensure(3 * sizeof(uint32_t) * ne + 16);
+            uint32_t* uniq   = runs.as<uint32_t>();
+            uint32_t* runcnt = uniq + ne;
+            uint32_t* runoff = runcnt + ne;
+            uint32_t* nruns  = runoff + ne;
+            VCHECK(vann::launch_edges(d_nodes, count, deg, adj, R, e_keys.as<uint32_t>(),
+                                      e_vals.as<uint32_t>(), nullptr, st));
+            size_t tmp_sort = 0, tmp_rle = 0, tmp_scan = 0;
+            VCHECK(cub::DeviceRadixSort::SortPairs(nullptr, tmp_sort, e_keys.as<uint32_t>(),
+                                                   e_keys2.as<uint32_t>(), e_vals.as<uint32_t>(),
+                                                   e_vals2.as<uint32_t>(), (int)ne, 0, end_bit, st));
+            VCHECK(cub::DeviceRunLengthEncode::Encode(nullptr, tmp_rle, e_keys2.as<uint32_t>(), uniq, runcnt,
+                                                      nruns, (int)ne, st));
+            VCHECK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_scan, runcnt, runoff, (int)ne, st));
+            cub_tmp.ensure(std::max(tmp_sort, std::max(tmp_rle, tmp_scan)));
+            size_t t1 = cub_tmp.bytes, t2 = cub_tmp.bytes, t3 = cub_tmp.bytes;
+            VCHECK(cub::DeviceRadixSort::SortPairs(cub_tmp.p, t1, e_keys.as<uint32_t>(),
+                                                   e_keys2.as<uint32_t>(), e_vals.as<uint32_t>(),
+                                                   e_vals2.as<uint32_t>(), (int)ne, 0, end_bit, st));
+            VCHECK(cub::DeviceRunLengthEncode::Encode(cub_tmp.p, t2, e_keys2.as<uint32_t>(), uniq, runcnt, nruns,
+                                                      (int)ne, st));
+            // runs beyond the count hold stale values; their offsets are never read
+            VCHECK(cub::DeviceScan::ExclusiveSum(cub_tmp.p, t3, runcnt, runoff, (int)ne, st));
+            uint32_t hn = 0;
+            VCHECK(cudaMemcpyAsync(&hn, nruns, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            VCHECK(cudaStreamSynchronize(st));
+            ra.node_ids    = uniq;  // the run of padded slots (id UINT32_MAX) is skipped
+            ra.n_nodes     = hn;
+            ra.csr_off     = runoff;
+            ra.csr_cnt     = runcnt;
+            ra.csr_by_slot = 1;
+            ra.skip_empty  = 0;
+            ra.consistent  = 1;
+        } else {
+            // lists of unknown origin: the reference's literal pass over every node
+            counts.ensure(sizeof(uint32_t) * (p.capacity + 1));
+            offsets.ensure(sizeof(uint32_t) * (p.capacity + 1));
+            VCHECK(cudaMemsetAsync(counts.p, 0, sizeof(uint32_t) * (size + 1), st));
+            VCHECK(vann::launch_edges(d_nodes, count, deg, adj, R, e_keys.as<uint32_t>(),
+                                      e_vals.as<uint32_t>(), counts.as<uint32_t>(), st));
+            size_t tmp_sort = 0, tmp_scan = 0;
+            VCHECK(cub::DeviceRadixSort::SortPairs(nullptr, tmp_sort, e_keys.as<uint32_t>(),
+                                                   e_keys2.as<uint32_t>(), e_vals.as<uint32_t>(),
+                                                   e_vals2.as<uint32_t>(), (int)ne, 0, end_bit, st));
+            VCHECK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_scan, counts.as<uint32_t>(),
+                                                 offsets.as<uint32_t>(), (int)(size + 1), st));
+            cub_tmp.ensure(std::max(tmp_sort, tmp_scan));
+            size_t t1 = cub_tmp.bytes, t2 = cub_tmp.bytes;
+            VCHECK(cub::DeviceRadixSort::SortPairs(cub_tmp.p, t1, e_keys.as<uint32_t>(),
+                                                   e_keys2.as<uint32_t>(), e_vals.as<uint32_t>(),
+                                                   e_vals2.as<uint32_t>(), (int)ne, 0, end_bit, st));
+            VCHECK(cub::DeviceScan::ExclusiveSum(cub_tmp.p, t2, counts.as<uint32_t>(),
+                                                 offsets.as<uint32_t>(), (int)(size + 1), st));
+            ra.node_ids   = nullptr;
+            ra.n_nodes    = size;
+            ra.csr_off    = offsets.as<uint32_t>();
+            ra.csr_cnt    = counts.as<uint32_t>();
+            ra.skip_empty = 0;
+            ra.consistent = 0;
+        }
+        ra.counter = next_counter(st);
         VCHECK(vann::launch_prune(ra, num_sms, st));
         consistent = true;
     }

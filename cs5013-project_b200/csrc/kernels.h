@@ -70,6 +70,7 @@ struct PruneArgs {
     const uint32_t* csr_off;
     const uint32_t* csr_cnt;
     const uint32_t* csr_src;
+    int             csr_by_slot; // csr_off / csr_cnt indexed by position in node_ids, not by id
     int             use_b;       // include the node's current out-neighbours
     int             skip_empty;  // re-prune: skip nodes without reverse entries
     int             consistent;  // B lists are alpha-consistent: skip B-B checks

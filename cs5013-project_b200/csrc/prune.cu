@@ -67,7 +67,8 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
         uint32_t mynode = 0;
         if (has) {
             mynode = a.node_ids ? __ldg(a.node_ids + wi) : wi;
-            if (rev && a.skip_empty && __ldg(a.csr_cnt + mynode) == 0u) has = false;
+            if (mynode == kNone) has = false;  // padded slots' run in the sorted edge list
+            if (has && rev && a.skip_empty && __ldg(a.csr_cnt + mynode) == 0u) has = false;
         }
         uint32_t todo = __ballot_sync(0xffffffffu, has);
         while (todo) {
@@ -82,8 +83,9 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
             // --- candidates: A then B
             uint32_t nA = 0, aoff = 0;
             if (rev) {
-                nA   = __ldg(a.csr_cnt + node);
-                aoff = __ldg(a.csr_off + node);
+                const uint32_t ci = a.csr_by_slot ? w : node;
+                nA   = __ldg(a.csr_cnt + ci);
+                aoff = __ldg(a.csr_off + ci);
                 nA   = min(nA, a.cap);
             } else {
                 nA = min(__ldg(a.a_n + w), a.a_stride);
