@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--duration", type=float, default=5.0, help="serve: seconds of arrivals")
     ap.add_argument("--write-frac", type=float, default=0.1, help="serve: share of write requests")
     ap.add_argument("--max-write", type=int, default=10_000, help="serve: largest write batch")
+    ap.add_argument("--commit-us", type=int, default=0,
+                    help="serve: group-commit interval in microseconds (0 = strict request order)")
     return ap.parse_args()
 
 
@@ -632,7 +634,9 @@ def main_serve():
     base = workload.mixture(n, DIM, clusters, seed=1)
     qpool = workload.mixture(20_000, DIM, clusters, seed=2)
     base_d = torch.from_numpy(base).to(dev)
-    cap = int(n * 1.05)
+    # room for every insert of the stream (deleted ids are reused only after a consolidate)
+    mean_write = (args.max_write - 1) / np.log(args.max_write) if args.max_write > 1 else 1.0
+    cap = n + int(1.5 * args.rate * args.duration * args.write_frac * 0.5 * mean_write) + 10_000
     idx = vann.Index(DIM, R, L_BUILD, ALPHA, capacity=cap, stores=("f32", "u8"))
     t0 = time.time()
     idx.build(base_d, batch=BATCH, seed=2024)
@@ -641,7 +645,7 @@ def main_serve():
     del base_d
     torch.cuda.empty_cache()
     srv = vann.Server(idx, max_batch=4096, slots=4, max_k=100, store="u8",
-                      hbm_budget=4 * 4096 * (DIM * 4 + 100 * 8 + 8))
+                      hbm_budget=4 * 4096 * (DIM * 4 + 100 * 8 + 8), commit_interval_us=args.commit_us)
     rng = np.random.default_rng(11)
     nreq = int(args.rate * args.duration)
     gaps = rng.exponential(1.0 / args.rate, nreq)
@@ -708,7 +712,9 @@ def main_serve():
                                    f"offered {args.rate:.0f} req/s for {args.duration} s; "
                                    f"{100 * (1 - args.write_frac):.0f}% searches k in {{1,10,100}}, "
                                    f"L in 16..512; writes log-uniform 1..{args.max_write}",
-                       "build_s": round(build_s, 2), "store": "u8"},
+                       "build_s": round(build_s, 2), "store": "u8",
+                       "write_order": (f"group commit every {args.commit_us} us" if args.commit_us
+                                       else "strict request order")},
             "offered_req_per_s": args.rate, "requests": nreq,
             "achieved_req_per_s": round(nreq / (t_end - t_start), 1),
             "submit_lag_s": round(t_submitted - t_start - float(gaps.sum()), 3),

@@ -13,6 +13,14 @@
 // done, so each search sees exactly the writes submitted before it, the same as
 // running the requests one by one.  Device memory for batches is fixed at
 // creation: the number of slots is capped by the HBM budget.
+//
+// With a commit interval (group commit), writes wait in their own queue while
+// searches keep being admitted against the last committed state; at most once
+// per interval (or as soon as no search is waiting) the in-flight batches drain
+// and every queued write is applied, in submission order.  Each request reports
+// its epoch: a search served at epoch e sees exactly the first e writes, so
+// replaying writes in order and running each search after its epoch's writes
+// reproduces every result.  One drain then serves many writes.
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -43,6 +51,7 @@ struct Request {
     Clock::time_point     t_submit, t_done;
     vann_status           status = VANN_OK;
     bool                  done   = false;
+    uint64_t              epoch  = 0;  // writes applied before this request was served
 };
 
 struct Slot {
@@ -67,6 +76,8 @@ struct vann_server {
     uint32_t             dim = 0;
     std::vector<Slot>    slots;
     std::deque<Request*> queue;
+    std::deque<Request*> wqueue;      // group commit: writes waiting for the next commit
+    uint64_t             epoch = 0;   // writes applied so far
     std::unordered_map<uint64_t, Request*> all;
     std::mutex              mu;
     std::condition_variable cv_work, cv_done;
@@ -133,6 +144,7 @@ struct vann_server {
             }
             kmax = r->k > kmax ? r->k : kmax;
             Lmax = r->L > Lmax ? r->L : Lmax;
+            r->epoch = epoch;
             s.reqs.emplace_back(r, rows);
             rows += r->n;
         }
@@ -198,33 +210,55 @@ struct vann_server {
         return st;
     }
 
+    void apply_write(std::unique_lock<std::mutex>& lk, Request* r) {
+        lk.unlock();
+        vann_status st = write(r);
+        lk.lock();
+        ++n_writes;
+        r->epoch = ++epoch;
+        complete(r, st);
+        cv_done.notify_all();
+    }
+
     void loop() {
         std::unique_lock<std::mutex> lk(mu);
+        const auto interval = std::chrono::microseconds(p.commit_interval_us);
         while (!stop) {
             harvest();
-            if (!queue.empty() && queue.front()->kind != kSearch) {
-                if (any_busy()) {  // earlier searches first
+            if (p.commit_interval_us == 0) {
+                // strict order: a write waits for the searches before it
+                if (!queue.empty() && queue.front()->kind != kSearch) {
+                    if (any_busy()) {
+                        cv_work.wait_for(lk, std::chrono::microseconds(20));
+                        continue;
+                    }
+                    Request* r = queue.front();
+                    queue.pop_front();
+                    apply_write(lk, r);
+                    continue;
+                }
+            } else if (!wqueue.empty() &&
+                       (queue.empty() || Clock::now() - wqueue.front()->t_submit >= interval)) {
+                // group commit: drain, then apply every queued write in order
+                if (any_busy()) {
                     cv_work.wait_for(lk, std::chrono::microseconds(20));
                     continue;
                 }
-                Request* r = queue.front();
-                queue.pop_front();
-                lk.unlock();
-                vann_status st = write(r);
-                lk.lock();
-                ++n_writes;
-                complete(r, st);
-                cv_done.notify_all();
+                for (size_t w = wqueue.size(); w > 0; --w) {  // writes queued by now
+                    Request* r = wqueue.front();
+                    wqueue.pop_front();
+                    apply_write(lk, r);
+                }
                 continue;
             }
             bool launched = false;
             for (Slot& s : slots)
                 if (!s.busy && !queue.empty() && queue.front()->kind == kSearch) launched |= admit(s);
             if (launched) continue;
-            if (any_busy())
-                cv_work.wait_for(lk, std::chrono::microseconds(20));  // poll the slot events
+            if (any_busy() || !wqueue.empty())
+                cv_work.wait_for(lk, std::chrono::microseconds(20));  // poll slot events / commit timer
             else
-                cv_work.wait(lk, [&] { return stop || !queue.empty(); });
+                cv_work.wait(lk, [&] { return stop || !queue.empty() || !wqueue.empty(); });
         }
     }
 
@@ -233,7 +267,10 @@ struct vann_server {
         r->ticket   = next_ticket++;
         r->t_submit = Clock::now();
         all[r->ticket] = r;
-        queue.push_back(r);
+        if (p.commit_interval_us > 0 && r->kind != kSearch)
+            wqueue.push_back(r);
+        else
+            queue.push_back(r);
         cv_work.notify_one();
         return r->ticket;
     }
@@ -365,7 +402,7 @@ vann_status vann_server_submit_consolidate(vann_server* s, uint64_t* ticket) {
 }
 
 vann_status vann_server_wait(vann_server* s, uint64_t ticket, uint32_t* h_ids, float* h_dists,
-                             double* latency_us, uint32_t timeout_ms) {
+                             double* latency_us, uint64_t* epoch, uint32_t timeout_ms) {
     if (!s) return VANN_ERR_INVALID;
     std::unique_lock<std::mutex> lk(s->mu);
     auto it = s->all.find(ticket);
@@ -378,6 +415,7 @@ vann_status vann_server_wait(vann_server* s, uint64_t ticket, uint32_t* h_ids, f
     if (h_dists && !r->out_d.empty()) memcpy(h_dists, r->out_d.data(), sizeof(float) * r->out_d.size());
     if (latency_us)
         *latency_us = std::chrono::duration<double, std::micro>(r->t_done - r->t_submit).count();
+    if (epoch) *epoch = r->epoch;
     vann_status st = r->status;
     if (st != VANN_OK) vann::set_last_error(s->last_error.c_str());
     s->all.erase(it);
@@ -394,7 +432,8 @@ vann_status vann_server_get_stats(vann_server* s, vann_server_stats* out) {
     out->queries      = s->n_searched;
     out->writes       = s->n_writes;
     out->max_inflight = s->max_inflight;
-    out->queued       = s->queue.size();
+    out->queued       = s->queue.size() + s->wqueue.size();
+    out->epoch        = s->epoch;
     return VANN_OK;
 }
 

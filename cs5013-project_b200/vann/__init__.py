@@ -62,13 +62,14 @@ class Info(C.Structure):
 
 class ServerParams(C.Structure):
     _fields_ = [("max_batch", C.c_uint32), ("slots", C.c_uint32), ("hbm_budget", C.c_uint64),
-                ("max_k", C.c_uint32), ("store", C.c_uint32), ("rerank", C.c_uint32)]
+                ("max_k", C.c_uint32), ("store", C.c_uint32), ("rerank", C.c_uint32),
+                ("commit_interval_us", C.c_uint32)]
 
 
 class ServerStats(C.Structure):
     _fields_ = [("slots", C.c_uint32), ("slot_bytes", C.c_uint64), ("batches", C.c_uint64),
                 ("queries", C.c_uint64), ("writes", C.c_uint64), ("max_inflight", C.c_uint64),
-                ("queued", C.c_uint64)]
+                ("queued", C.c_uint64), ("epoch", C.c_uint64)]
 
 
 _lib = None
@@ -112,7 +113,7 @@ def lib():
             "vann_server_submit_insert": (C.c_int, [vp, vp, u32, C.POINTER(u64)]),
             "vann_server_submit_delete": (C.c_int, [vp, vp, u32, C.POINTER(u64)]),
             "vann_server_submit_consolidate": (C.c_int, [vp, C.POINTER(u64)]),
-            "vann_server_wait": (C.c_int, [vp, u64, vp, vp, C.POINTER(C.c_double), u32]),
+            "vann_server_wait": (C.c_int, [vp, u64, vp, vp, C.POINTER(C.c_double), C.POINTER(u64), u32]),
             "vann_server_get_stats": (C.c_int, [vp, C.POINTER(ServerStats)]),
         }
         for name, (res, args) in sig.items():
@@ -300,8 +301,8 @@ class Server:
     carry host (numpy) data; submit_* return tickets, wait() returns results."""
 
     def __init__(self, index: "Index", max_batch: int = 4096, slots: int = 4, hbm_budget: int = 0,
-                 max_k: int = 100, store: str = "f32", rerank: bool = False):
-        p = ServerParams(max_batch, slots, hbm_budget, max_k, STORES[store], int(rerank))
+                 max_k: int = 100, store: str = "f32", rerank: bool = False, commit_interval_us: int = 0):
+        p = ServerParams(max_batch, slots, hbm_budget, max_k, STORES[store], int(rerank), commit_interval_us)
         h = C.c_void_p()
         _check(lib().vann_server_create(index._h, C.byref(p), C.byref(h)))
         self._h, self.index, self.dim = h, index, index.dim
@@ -348,16 +349,19 @@ class Server:
         self._kind[t.value] = ("consolidate", 0, 0)
         return t.value
 
-    def wait(self, ticket: int, timeout_ms: int = 0):
-        """-> (ids, dists, latency_us); ids/dists are n x k for searches, the new ids for inserts."""
+    def wait(self, ticket: int, timeout_ms: int = 0, with_epoch: bool = False):
+        """-> (ids, dists, latency_us[, epoch]); ids/dists are n x k for searches, the new
+        ids for inserts; epoch = writes a search saw / a write's position in the write order."""
         import numpy as np
         kind, n, k = self._kind.pop(ticket)
         ids = np.empty((n, k), np.uint32) if kind == "search" else np.empty(n, np.uint32)
         d = np.empty((n, k), np.float32) if kind == "search" else None
         lat = C.c_double()
+        ep = C.c_uint64()
         _check(lib().vann_server_wait(self._h, ticket, ids.ctypes.data if n else None,
-                                      d.ctypes.data if d is not None else None, C.byref(lat), timeout_ms))
-        return ids, d, lat.value
+                                      d.ctypes.data if d is not None else None, C.byref(lat), C.byref(ep),
+                                      timeout_ms))
+        return (ids, d, lat.value, ep.value) if with_epoch else (ids, d, lat.value)
 
     def stats(self) -> dict:
         s = ServerStats()

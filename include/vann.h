@@ -195,12 +195,15 @@ typedef struct {
     uint32_t max_k;       /* largest k a search may ask for */
     uint32_t store;       /* vann_store searches traverse */
     uint32_t rerank;      /* exact FP32 rerank */
+    uint32_t commit_interval_us; /* 0: strict request order; > 0: group commit of writes at most
+                                    this often, searches served at the last committed epoch */
 } vann_server_params;
 
 typedef struct {
     uint32_t slots;        /* slots admitted under the budget */
     uint64_t slot_bytes;   /* device bytes per slot */
     uint64_t batches, queries, writes, max_inflight, queued;
+    uint64_t epoch;        /* writes applied so far */
 } vann_server_stats;
 
 typedef struct vann_server vann_server;
@@ -214,9 +217,11 @@ vann_status vann_server_submit_insert(vann_server* server, const float* h_vecs, 
 vann_status vann_server_submit_delete(vann_server* server, const uint32_t* h_ids, uint32_t n, uint64_t* ticket);
 vann_status vann_server_submit_consolidate(vann_server* server, uint64_t* ticket);
 /* Blocks until the request is done (timeout_ms 0 = 10 minutes).  Search: n x k ids
- * and distances; insert: the n new ids in h_ids.  latency_us: submit to done. */
+ * and distances; insert: the n new ids in h_ids.  latency_us: submit to done.
+ * epoch: for a search, the number of writes it saw; for a write, its position in
+ * the order writes were applied (1-based).  Any out pointer may be NULL. */
 vann_status vann_server_wait(vann_server* server, uint64_t ticket, uint32_t* h_ids, float* h_dists,
-                             double* latency_us, uint32_t timeout_ms);
+                             double* latency_us, uint64_t* epoch, uint32_t timeout_ms);
 vann_status vann_server_get_stats(vann_server* server, vann_server_stats* out);
 
 /* Allocation-free entry-point selection.  No counterpart in the reference.

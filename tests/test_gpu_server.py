@@ -83,3 +83,71 @@ def test_server_budget_caps_slots(vann_mod):
     srv.close()
     with pytest.raises(vann_mod.VannError):
         vann_mod.Server(idx, max_batch=64, slots=8, max_k=10, hbm_budget=slot - 1)
+
+
+def test_group_commit_replays_by_epoch(vann_mod):
+    """Group commit: searches flow past queued writes and report the epoch (number of
+    writes applied) they were served at; writes are applied in submission order.
+    Replaying the writes in order on an identical index and running each search after
+    its epoch's writes gives bit-identical results."""
+    import torch
+
+    base = workload.mixture(8000, 128, 30, seed=83)
+    served, alone = _index(vann_mod, base), _index(vann_mod, base)
+    srv = vann_mod.Server(served, max_batch=256, slots=4, max_k=100, commit_interval_us=3000)
+    rng = np.random.default_rng(6)
+    ops, live = [], list(range(len(base)))
+    for i in range(400):
+        u = rng.random()
+        if u < 0.88:
+            k = int(rng.choice([1, 10, 100]))
+            ops.append(("search", workload.mixture(int(rng.integers(1, 5)), 128, 30, seed=30_000 + i),
+                        k, max(k, int(rng.integers(16, 257)))))
+        elif u < 0.94:
+            ops.append(("insert", workload.mixture(int(rng.integers(1, 40)), 128, 30, seed=40_000 + i)))
+        elif u < 0.99:
+            pick = set(rng.choice(len(live), int(rng.integers(1, 20)), replace=False).tolist())
+            ops.append(("delete", np.array([live[j] for j in sorted(pick)], np.uint32)))
+            live = [x for j, x in enumerate(live) if j not in pick]
+        else:
+            ops.append(("consolidate",))
+    tickets = []
+    for op in ops:
+        if op[0] == "search":
+            tickets.append(srv.submit_search(op[1], op[2], op[3]))
+        elif op[0] == "insert":
+            tickets.append(srv.submit_insert(op[1]))
+        elif op[0] == "delete":
+            tickets.append(srv.submit_delete(op[1]))
+        else:
+            tickets.append(srv.submit_consolidate())
+    results = [srv.wait(t, with_epoch=True) for t in tickets]
+    st = srv.stats()
+    srv.close()
+    writes = [i for i, op in enumerate(ops) if op[0] != "search"]
+    assert st["writes"] == len(writes) and st["epoch"] == len(writes)
+    # writes were applied in submission order: the j-th write has epoch j + 1
+    assert [results[i][3] for i in writes] == list(range(1, len(writes) + 1))
+    searches = [i for i, op in enumerate(ops) if op[0] == "search"]
+    assert all(0 <= results[i][3] <= len(writes) for i in searches)
+    assert st["batches"] < len(searches)
+
+    by_epoch = {}
+    for i in searches:
+        by_epoch.setdefault(results[i][3], []).append(i)
+    for e in range(len(writes) + 1):
+        for i in by_epoch.get(e, []):
+            op, (ids, d, _, _) = ops[i], results[i]
+            gi, gd = alone.search(torch.from_numpy(op[1]).cuda(), k=op[2], L=op[3])
+            assert np.array_equal(ids, gi.cpu().numpy().view(np.uint32))
+            assert np.array_equal(d, gd.cpu().numpy())
+        if e == len(writes):
+            break
+        op, res = ops[writes[e]], results[writes[e]]
+        if op[0] == "insert":
+            new = alone.insert(torch.from_numpy(op[1]).cuda()).cpu().numpy().view(np.uint32)
+            assert np.array_equal(res[0], new)
+        elif op[0] == "delete":
+            alone.delete(torch.from_numpy(op[1].astype(np.int32)).cuda())
+        else:
+            alone.consolidate()
