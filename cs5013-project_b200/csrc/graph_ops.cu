@@ -62,7 +62,7 @@ cudaError_t launch_hash_rows(const uint32_t* adj, uint32_t* adj_h, uint64_t n, u
 // FP32 rows -> traversal copies.  FP8: scale = amax / 448 per row (e4m3 max
 // finite 448), codes = satfinite(x / scale).  U8: round to nearest, clamp.
 __global__ void convert_kernel(const float* src, void* dst, float* scale, uint64_t rows, uint32_t D,
-                               int store) {
+                               int store, uint32_t* inexact) {
     uint64_t r    = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
     uint32_t lane = threadIdx.x & 31u;
     if (r >= rows) return;
@@ -81,26 +81,29 @@ __global__ void convert_kernel(const float* src, void* dst, float* scale, uint64
             d[i] = (uint8_t)__nv_cvt_float_to_fp8(s[i] * inv, __NV_SATFINITE, __NV_E4M3);
         if (lane == 0) scale[r] = sc;
     } else if (store == 3) {
-        uint8_t* d = static_cast<uint8_t*>(dst) + r * D;
+        uint8_t* d   = static_cast<uint8_t*>(dst) + r * D;
+        bool     off = false;
         for (uint32_t i = lane; i < D; i += 32) {
             float v = rintf(s[i]);
             v       = fminf(fmaxf(v, 0.f), 255.f);
             d[i]    = (uint8_t)v;
+            off |= !(v == s[i]);
         }
+        if (__any_sync(0xffffffffu, off) && lane == 0) atomicOr(inexact, 1u);
     }
 }
 
 cudaError_t launch_convert(const float* src, void* dst, float* scale, uint64_t rows, uint32_t D,
-                           int store, cudaStream_t st) {
+                           int store, uint32_t* inexact, cudaStream_t st) {
     if (rows == 0) return cudaSuccess;
-    convert_kernel<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(src, dst, scale, rows, D, store);
+    convert_kernel<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(src, dst, scale, rows, D, store, inexact);
     return cudaGetLastError();
 }
 
 // Same conversion for rows scattered over an id list (inserts into reused ids):
 // one warp per listed row, the row's traversal copy rewritten from its FP32 row.
 __global__ void convert_ids_kernel(const float* vecs, const uint32_t* ids, uint64_t n, void* dst,
-                                   float* scale, uint32_t D, int store) {
+                                   float* scale, uint32_t D, int store, uint32_t* inexact) {
     uint64_t i    = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
     uint32_t lane = threadIdx.x & 31u;
     if (i >= n) return;
@@ -120,14 +123,20 @@ __global__ void convert_ids_kernel(const float* vecs, const uint32_t* ids, uint6
             d[k] = (uint8_t)__nv_cvt_float_to_fp8(s[k] * inv, __NV_SATFINITE, __NV_E4M3);
         if (lane == 0) scale[r] = sc;
     } else if (store == 3) {
-        uint8_t* d = static_cast<uint8_t*>(dst) + r * D;
-        for (uint32_t k = lane; k < D; k += 32) d[k] = (uint8_t)fminf(fmaxf(rintf(s[k]), 0.f), 255.f);
+        uint8_t* d   = static_cast<uint8_t*>(dst) + r * D;
+        bool     off = false;
+        for (uint32_t k = lane; k < D; k += 32) {
+            const float v = fminf(fmaxf(rintf(s[k]), 0.f), 255.f);
+            d[k]          = (uint8_t)v;
+            off |= !(v == s[k]);
+        }
+        if (__any_sync(0xffffffffu, off) && lane == 0) atomicOr(inexact, 1u);
     }
 }
 cudaError_t launch_convert_ids(const float* vecs, const uint32_t* ids, uint64_t n, void* dst, float* scale,
-                               uint32_t D, int store, cudaStream_t st) {
+                               uint32_t D, int store, uint32_t* inexact, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
-    convert_ids_kernel<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(vecs, ids, n, dst, scale, D, store);
+    convert_ids_kernel<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(vecs, ids, n, dst, scale, D, store, inexact);
     return cudaGetLastError();
 }
 

@@ -138,7 +138,7 @@ struct vann_index {
         return it == tuned.end() ? 0 : it->second;
     }
 
-    DevBuf vis_ids, vis_d, vis_n, nodes, runs, e_keys, e_vals, e_keys2, e_vals2, counts, offsets, cub_tmp,
+    DevBuf vis_ids, vis_d, vis_n, nodes, runs, ovf, e_keys, e_vals, e_keys2, e_vals2, counts, offsets, cub_tmp,
         medoid_ws, gather, cand, cand_n, cand_d, list_n, out_tmp;
 
     void alloc(void** ptr, size_t bytes) {
@@ -155,7 +155,7 @@ struct vann_index {
         cudaFree(tomb);
         cudaFree(counters);
         cudaFree(status);
-        for (DevBuf* b : {&vis_ids, &vis_d, &vis_n, &nodes, &runs, &e_keys, &e_vals, &e_keys2, &e_vals2,
+        for (DevBuf* b : {&vis_ids, &vis_d, &vis_n, &nodes, &runs, &ovf, &e_keys, &e_vals, &e_keys2, &e_vals2,
                           &counts, &offsets, &cub_tmp, &medoid_ws, &gather, &cand, &cand_n, &cand_d,
                           &list_n, &out_tmp})
             b->release();
@@ -169,13 +169,47 @@ struct vann_index {
 
     uint64_t tomb_words() const { return (p.capacity + 31) / 32; }
 
+    uint32_t* u8_inexact() const { return status + vann::kWordU8Inexact; }
+
+    // rows [first, first + rows) -> traversal copies; rows from 0 replace every
+    // row, so the uint8 exactness flag starts over
     void convert_rows(uint64_t first, uint64_t rows, cudaStream_t st) {
+        if (first == 0) VCHECK(cudaMemsetAsync(u8_inexact(), 0, sizeof(uint32_t), st));
         for (int s = 1; s < 4; ++s) {
             if (!store[s]) continue;
             size_t esz = s == 1 ? 2 : 1;
             void*  dst = static_cast<char*>(store[s]) + first * p.dim * esz;
             VCHECK(vann::launch_convert(vecs + first * p.dim, dst, s == 2 ? fp8_scale + first : nullptr,
-                                        rows, p.dim, s, st));
+                                        rows, p.dim, s, u8_inexact(), st));
+        }
+    }
+
+    // RobustPrune launch: the tensor-core pass when an exact uint8 copy exists
+    // (decided on the device by the exactness flag), prune_kernel for the rest
+    void run_prune(vann::PruneArgs pa, cudaStream_t st) {
+        if (pa.n_nodes == 0) return;
+        pa.pruned = reinterpret_cast<unsigned long long*>(status + vann::kWordPruned);
+        if (store[3] && vann::prune_tc_supported(p.dim, p.degree)) {
+            ovf.ensure(sizeof(uint32_t) * (3 * pa.n_nodes + 4));
+            pa.vecs_u8  = static_cast<const uint8_t*>(store[3]);
+            pa.gate     = u8_inexact();
+            pa.in_list  = ovf.as<uint32_t>();
+            pa.in_count = status + vann::kWordOverflow;
+            uint32_t* tc_counters = next_counter(st);  // [0] first pass, [1] second pass
+            VCHECK(cudaMemsetAsync(tc_counters + 1, 0, sizeof(uint32_t), st));
+            VCHECK(vann::launch_prune_tc(pa, ovf.as<uint32_t>() + pa.n_nodes, tc_counters, num_sms, st));
+            pa.counter = next_counter(st);
+        }
+        VCHECK(vann::launch_prune(pa, num_sms, st));
+    }
+
+    // a bounded device wait that gave up is reported by the call that launched it
+    void check_device_status() {
+        uint32_t w = 0;
+        VCHECK(cudaMemcpy(&w, status, sizeof(w), cudaMemcpyDeviceToHost));
+        if (w & vann::kStatusTimeout) {
+            VCHECK(cudaMemset(status, 0, sizeof(uint32_t)));
+            VREQUIRE(false, VANN_ERR_TIMEOUT, "a bounded device wait gave up (tensor-core prune)");
         }
     }
 
@@ -247,7 +281,7 @@ struct vann_index {
         pa.consistent = 0;
         pa.counter = next_counter(st);
         pa.status = status;
-        VCHECK(vann::launch_prune(pa, num_sms, st));
+        run_prune(pa, st);
 
         // reverse edges, sorted by target with sources in batch order (stable)
         const uint64_t ne             = count * R;
@@ -334,7 +368,7 @@ struct vann_index {
             ra.consistent = 0;
         }
         ra.counter = next_counter(st);
-        VCHECK(vann::launch_prune(ra, num_sms, st));
+        run_prune(ra, st);
         consistent = true;
     }
 };
@@ -455,6 +489,10 @@ vann_status vann_get_info(const vann_index* h, vann_info* out) {
         out->degree = h->p.degree;
         out->consistent = h->consistent ? 1u : 0u;
         out->device_bytes = h->held;
+        unsigned long long pr[2] = {0, 0};
+        VCHECK(cudaMemcpy(pr, h->status + vann::kWordPruned, sizeof(pr), cudaMemcpyDeviceToHost));
+        out->pruned_tc   = pr[0];
+        out->pruned_cuda = pr[1];
     });
 }
 
@@ -584,6 +622,7 @@ vann_status vann_build(vann_index* h, const float* d_vecs, uint64_t n, uint64_t 
         }
         VCHECK(cudaStreamSynchronize(st));
         VCHECK(cudaGetLastError());
+        h->check_device_status();
     });
 }
 
@@ -598,6 +637,7 @@ vann_status vann_build_loaded(vann_index* h, void* stream) {
         VCHECK(vann::launch_iota(h->nodes.as<uint32_t>(), h->size, 0, st));
         h->vamana_batch(h->nodes.as<uint32_t>(), h->size, h->vecs, parity ? 1u : 2u, 0u, true, st);
         VCHECK(cudaStreamSynchronize(st));
+        h->check_device_status();
     });
 }
 
@@ -709,7 +749,10 @@ vann_status vann_sync(vann_index* h, void* stream) {
         uint32_t w = 0;
         VCHECK(cudaMemcpy(&w, h->status, sizeof(w), cudaMemcpyDeviceToHost));
         VCHECK(cudaMemset(h->status, 0, sizeof(uint32_t)));
-        if (w & vann::kStatusHopLimit) {
+        if (w & vann::kStatusTimeout) {
+            set_err("a bounded device wait gave up");
+            result = VANN_ERR_TIMEOUT;
+        } else if (w & vann::kStatusHopLimit) {
             set_err("a search stopped at its hop limit");
             result = VANN_ERR_HOP_LIMIT;
         }
@@ -744,7 +787,7 @@ vann_status vann_insert(vann_index* h, const float* d_vecs, uint64_t n, uint32_t
             for (int s = 1; s < 4; ++s)  // reused ids are scattered: convert by id list
                 if (h->store[s])
                     VCHECK(vann::launch_convert_ids(h->vecs, h->nodes.as<uint32_t>(), n, h->store[s],
-                                                    s == 2 ? h->fp8_scale : nullptr, D, s, st));
+                                                    s == 2 ? h->fp8_scale : nullptr, D, s, h->u8_inexact(), st));
         }
         h->size += n - reuse;
         const bool parity = (h->p.flags & VANN_QUIRK_SKIP_BATCH_INDEX) != 0;
@@ -752,6 +795,7 @@ vann_status vann_insert(vann_index* h, const float* d_vecs, uint64_t n, uint32_t
         if (d_ids_out)
             VCHECK(cudaMemcpyAsync(d_ids_out, h->nodes.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
         VCHECK(cudaStreamSynchronize(st));
+        h->check_device_status();
     });
 }
 
@@ -842,7 +886,7 @@ vann_status vann_consolidate(vann_index* h, void* stream) {
         pa.consistent = 0;
         pa.counter = h->next_counter(st);
         pa.status = h->status;
-        VCHECK(vann::launch_prune(pa, h->num_sms, st));
+        h->run_prune(pa, st);
         // free the deleted ids (tombstone stays set until an insert reuses the id)
         h->nodes.ensure(sizeof(uint32_t) * std::max<size_t>(dead.size(), h->size));
         VCHECK(cudaMemcpyAsync(h->nodes.p, dead.data(), sizeof(uint32_t) * dead.size(),
@@ -897,6 +941,7 @@ vann_status vann_consolidate(vann_index* h, void* stream) {
         for (uint32_t d : dead) h->free_ids.push_back(d);
         h->n_deleted = 0;
         VCHECK(cudaStreamSynchronize(st));
+        h->check_device_status();
     });
 }
 

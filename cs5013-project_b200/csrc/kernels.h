@@ -76,19 +76,31 @@ struct PruneArgs {
     int             consistent;  // B lists are alpha-consistent: skip B-B checks
     uint32_t*       counter;     // work counter, zeroed before launch
     uint32_t*       status;
+    // tensor-core passes (prune_tc.cu) and their hand-off to prune_kernel
+    const uint8_t*  vecs_u8;     // exact uint8 rows
+    const uint32_t* gate;        // non-zero: the uint8 rows are not exact
+    uint32_t*       in_list;     // slots (positions in node_ids) left to prune_kernel
+    uint32_t*       in_count;
+    unsigned long long* pruned;  // [0] tensor-core, [1] CUDA-core node counts (or null)
 };
 
+// prune_kernel: with gate == null every node; otherwise every node when *gate
+// is set, else only the in_list slots the tensor-core passes handed over.
 cudaError_t launch_prune(const PruneArgs& a, int num_sms, cudaStream_t st);
+bool        prune_tc_supported(uint32_t D, uint32_t R);
+// ws: 2 * n_nodes + 4 words of scratch; counters: two zeroed work counters
+cudaError_t launch_prune_tc(const PruneArgs& a, uint32_t* ws, uint32_t* counters, int num_sms, cudaStream_t st);
 
 // graph utilities (graph_ops.cu)
 cudaError_t launch_random_graph(uint32_t* deg, uint32_t* adj, uint32_t* adj_h, uint64_t first,
                                 uint64_t n, uint32_t R, uint64_t seed, cudaStream_t st);
 cudaError_t launch_hash_rows(const uint32_t* adj, uint32_t* adj_h, uint64_t n, uint32_t R,
                              cudaStream_t st);
+// inexact: set non-zero when a uint8 code is not exactly its FP32 value
 cudaError_t launch_convert(const float* src, void* dst, float* scale, uint64_t rows, uint32_t D,
-                           int store, cudaStream_t st);
+                           int store, uint32_t* inexact, cudaStream_t st);
 cudaError_t launch_convert_ids(const float* vecs, const uint32_t* ids, uint64_t n, void* dst, float* scale,
-                               uint32_t D, int store, cudaStream_t st);
+                               uint32_t D, int store, uint32_t* inexact, cudaStream_t st);
 cudaError_t launch_iota(uint32_t* out, uint64_t n, uint32_t first, cudaStream_t st);
 cudaError_t launch_set_bits(uint32_t* bits, const uint32_t* ids, uint64_t n, uint64_t limit,
                             cudaStream_t st);

@@ -17,6 +17,8 @@
 // same alpha, kept in selection order), a B candidate can never be pruned by a
 // B p*, so those pairs are not evaluated: the decisions are the same, the
 // distance evaluations drop from |C|^2 to about |A| * |C|.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -39,7 +41,8 @@ struct PruneLayout {
 };
 
 template <int DC>
-__global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, uint32_t warp_bytes) {
+__global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, uint32_t warp_bytes,
+                                                    uint32_t chunk) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t wib  = threadIdx.x >> 5;
@@ -53,28 +56,35 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
     const uint32_t R    = a.R;
     uint32_t*      plist  = chosen + R;  // positions of one round's candidates
     const bool     rev  = a.csr_off != nullptr;
-    const uint32_t chunk = 32u;
+    // paired with the tensor-core passes: all nodes if they stood down, else the
+    // large nodes they handed over, one per warp
+    const bool     all   = a.gate == nullptr || *reinterpret_cast<volatile const uint32_t*>(a.gate) != 0u;
+    const uint64_t nwork = all ? a.n_nodes : (uint64_t)*reinterpret_cast<volatile const uint32_t*>(a.in_count);
+    if (!all) chunk = 1u;
 
+    uint32_t done = 0;  // nodes pruned by this warp
     for (;;) {
         uint32_t w0 = 0;
         if (lane == 0) w0 = atomicAdd(a.counter, chunk);
         w0 = __shfl_sync(0xffffffffu, w0, 0);
-        if (w0 >= a.n_nodes) break;
-        uint32_t wend = (uint32_t)min((uint64_t)w0 + chunk, a.n_nodes);
+        if (w0 >= nwork) break;
+        uint32_t wend = (uint32_t)min((uint64_t)w0 + chunk, nwork);
         // which of the chunk's nodes have work
         uint32_t wi   = w0 + lane;
-        bool     has  = wi < wend;
-        uint32_t mynode = 0;
+        bool     has  = lane < chunk && wi < wend;
+        uint32_t myslot = 0, mynode = 0;
         if (has) {
-            mynode = a.node_ids ? __ldg(a.node_ids + wi) : wi;
+            myslot = all ? wi : __ldg(a.in_list + wi);
+            mynode = a.node_ids ? __ldg(a.node_ids + myslot) : myslot;
             if (mynode == kNone) has = false;  // padded slots' run in the sorted edge list
-            if (has && rev && a.skip_empty && __ldg(a.csr_cnt + mynode) == 0u) has = false;
+            if (has && rev && a.skip_empty && __ldg(a.csr_cnt + (a.csr_by_slot ? myslot : mynode)) == 0u)
+                has = false;
         }
         uint32_t todo = __ballot_sync(0xffffffffu, has);
         while (todo) {
             const uint32_t src  = __ffs(todo) - 1u;
             todo &= todo - 1u;
-            const uint32_t w    = w0 + src;
+            const uint32_t w    = __shfl_sync(0xffffffffu, myslot, src);
             const uint32_t node = __shfl_sync(0xffffffffu, mynode, src);
 
             Query<StoreF32, DC> nv;
@@ -159,8 +169,10 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
                 __syncwarp();
                 if (ndeg >= R) break;
 
+                // p*'s row is fetched only if some candidate needs its distance
+                // (with consistent B lists a B p* only checks the A candidates)
                 Query<StoreF32, DC> pv;
-                load_query<StoreF32, DC>(pv, a.vecs + (uint64_t)ps * a.D, a.D, lane);
+                bool                have_pv = false;
                 for (uint32_t c0 = first; c0 < ncap; c0 += 32) {
                     uint32_t i    = c0 + lane;
                     bool     need = false;
@@ -171,6 +183,10 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
                     uint32_t m  = __ballot_sync(0xffffffffu, need);
                     uint32_t nm = __popc(m);
                     if (nm == 0) continue;
+                    if (!have_pv) {
+                        load_query<StoreF32, DC>(pv, a.vecs + (uint64_t)ps * a.D, a.D, lane);
+                        have_pv = true;
+                    }
                     if (need) plist[__popc(m & ((1u << lane) - 1u))] = i;
                     __syncwarp();
                     for (uint32_t g0 = 0; g0 < nm; g0 += G) {
@@ -193,8 +209,10 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
             }
             if (lane == 0) a.deg[node] = ndeg;
             __syncwarp();
+            ++done;
         }
     }
+    if (lane == 0 && a.pruned && done) atomicAdd(a.pruned + 1, (unsigned long long)done);
 }
 
 cudaError_t launch_prune(const PruneArgs& a, int num_sms, cudaStream_t st) {
@@ -203,7 +221,7 @@ cudaError_t launch_prune(const PruneArgs& a, int num_sms, cudaStream_t st) {
     PruneLayout lay  = PruneLayout::make(maxa + a.R, a.R);
     const int   warps = 4;
     size_t      smem  = (size_t)lay.bytes * warps;
-    void (*kern)(PruneArgs, uint32_t, uint32_t);
+    void (*kern)(PruneArgs, uint32_t, uint32_t, uint32_t);
     if (a.D <= 128)
         kern = prune_kernel<0>;
     else if (a.D <= 256)
@@ -219,10 +237,14 @@ cudaError_t launch_prune(const PruneArgs& a, int num_sms, cudaStream_t st) {
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    uint64_t need = (a.n_nodes + 32 * warps - 1) / (32 * warps);
+    // nodes per counter grab: up to 32, fewer when the launch has too few nodes to
+    // give every resident warp work (each warp prunes its nodes one after another)
+    const uint64_t resident = (uint64_t)per_sm * num_sms * warps;
+    uint32_t       chunk    = (uint32_t)std::min<uint64_t>(32, std::max<uint64_t>(1, a.n_nodes / (4 * resident)));
+    uint64_t need = (a.n_nodes + (uint64_t)chunk * warps - 1) / ((uint64_t)chunk * warps);
     uint64_t grid = (uint64_t)per_sm * num_sms;
     if (grid > need) grid = need;
-    kern<<<(unsigned)grid, warps * 32, smem, st>>>(a, lay.p2, lay.bytes);
+    kern<<<(unsigned)grid, warps * 32, smem, st>>>(a, lay.p2, lay.bytes, chunk);
     return cudaGetLastError();
 }
 

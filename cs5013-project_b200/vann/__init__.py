@@ -57,7 +57,8 @@ class SearchParams(C.Structure):
 class Info(C.Structure):
     _fields_ = [("size", C.c_uint64), ("capacity", C.c_uint64), ("live", C.c_uint64),
                 ("free_ids", C.c_uint64), ("entry", C.c_uint32), ("dim", C.c_uint32),
-                ("degree", C.c_uint32), ("consistent", C.c_uint32), ("device_bytes", C.c_uint64)]
+                ("degree", C.c_uint32), ("consistent", C.c_uint32), ("device_bytes", C.c_uint64),
+                ("pruned_tc", C.c_uint64), ("pruned_cuda", C.c_uint64)]
 
 
 class ServerParams(C.Structure):

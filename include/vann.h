@@ -82,6 +82,8 @@ typedef struct {
     uint32_t dim, degree;
     uint32_t consistent;   /* 1 when every adjacency list came from RobustPrune with alpha */
     uint64_t device_bytes; /* device memory held by the index */
+    uint64_t pruned_tc;    /* RobustPrune runs done with the Gram matrix on the tensor cores */
+    uint64_t pruned_cuda;  /* RobustPrune runs done on the CUDA cores (float rows, overflow) */
 } vann_info;
 
 typedef struct vann_index vann_index;

@@ -1,0 +1,120 @@
+"""Tensor-core RobustPrune (prune_tc.cu): with an exact uint8 copy the Gram matrix
+of each node's candidates comes from tcgen05.mma, and every graph it builds must be
+bit-identical to the CUDA-core path and to the CPU oracle."""
+import numpy as np
+import pytest
+
+from vann import workload
+
+pytestmark = pytest.mark.gpu
+
+
+def _rows_equal(deg_a, adj_a, deg_b, adj_b):
+    return [i for i in range(len(deg_a)) if not np.array_equal(adj_a[i, :deg_a[i]], adj_b[i, :deg_b[i]])]
+
+
+def _build(vann_mod, base, R, L, stores, batch=0, seed=7, quirks=0, alpha=1.2):
+    import torch
+
+    idx = vann_mod.Index(base.shape[1], R, L, alpha, capacity=len(base) + 1000, stores=stores, quirks=quirks)
+    idx.build(torch.from_numpy(base).cuda(), batch=batch, seed=seed)
+    return idx
+
+
+@pytest.mark.parametrize("R,L", [(32, 75), (64, 100)])
+def test_one_batch_build_matches_oracle(oracle, vann_mod, R, L):
+    base = workload.mixture(3000, 128, 30, seed=41)
+    og, entry = oracle.build_index(base, R=R, L=L, alpha=1.2, seed=7, skip_mode=2,
+                                   bloom_mode=oracle.BLOOM_SNAPSHOT)
+    idx = _build(vann_mod, base, R, L, ("f32", "u8"))
+    info = idx.info()
+    assert info["entry"] == entry
+    assert info["pruned_tc"] > 0
+    _, deg, adj = idx.get_graph()
+    assert _rows_equal(deg, adj, og.deg, og.adj) == []
+
+
+def test_batched_build_and_insert_equal_cuda_core_path(vann_mod):
+    import torch
+
+    base = workload.mixture(6000, 128, 40, seed=42)
+    extra = workload.mixture(700, 128, 40, seed=43)
+    tc = _build(vann_mod, base, 64, 100, ("f32", "u8"), batch=1000, seed=3)
+    cc = _build(vann_mod, base, 64, 100, ("f32",), batch=1000, seed=3)
+    assert tc.info()["pruned_tc"] > 0 and cc.info()["pruned_tc"] == 0
+    for idx in (tc, cc):
+        for s in range(0, 700, 233):  # uneven insert batches
+            idx.insert(torch.from_numpy(extra[s:s + 233]).cuda())
+    _, da, aa = tc.get_graph()
+    _, db, ab = cc.get_graph()
+    assert _rows_equal(da, aa, db, ab) == []
+
+
+def test_loaded_start_graph_two_tiles(oracle, vann_mod):
+    """runVamana over a loaded R=64 start graph: expansion lists of ~L plus 64
+    out-neighbours give 129..256 candidates, i.e. two 128-row tiles."""
+    n, R, L = 3000, 64, 150
+    base = workload.mixture(n, 128, 30, seed=44)
+    rng = np.random.default_rng(6)
+    adj = rng.integers(0, n, (n, R)).astype(np.uint32)
+    deg = np.full(n, R, np.uint32)
+    entry = 1200
+    og = oracle.Graph(base, deg.copy(), adj.copy())
+    assert og.vamana_batch(0, n, L, 1.5, entry, 600, 500, skip_mode=1, bloom_mode=oracle.BLOOM_SNAPSHOT) == 0
+    idx = vann_mod.Index(128, R, L, 1.5, capacity=n, quirks=vann_mod.QUIRK_SKIP_BATCH_INDEX, stores=("f32", "u8"))
+    idx.set_graph(base, deg, adj, entry)
+    idx.build_loaded()
+    assert idx.info()["pruned_tc"] > 0
+    _, gdeg, gadj = idx.get_graph()
+    assert _rows_equal(gdeg, gadj, og.deg, og.adj) == []
+
+
+@pytest.mark.parametrize("L,max_visited,cuda_share", [(300, 600, False), (600, 800, True)])
+def test_large_candidate_lists(oracle, vann_mod, L, max_visited, cuda_share):
+    """257..512 candidates (expansion lists at L=300) take the second tensor-core
+    pass; more than 512 (L=600) are handed to the CUDA-core kernel.  Either way the
+    graph is the oracle's."""
+    import torch
+
+    base = workload.mixture(2500, 128, 20, seed=45)
+    og, entry = oracle.build_index(base, R=32, L=L, alpha=1.2, seed=9, skip_mode=2,
+                                   bloom_mode=oracle.BLOOM_SNAPSHOT, max_visited=max_visited)
+    idx = vann_mod.Index(128, 32, L, 1.2, capacity=2500, max_visited=max_visited, stores=("f32", "u8"))
+    idx.build(torch.from_numpy(base).cuda(), batch=0, seed=9)
+    info = idx.info()
+    assert info["pruned_tc"] > 0
+    if cuda_share:
+        assert info["pruned_cuda"] > 0
+    _, deg, adj = idx.get_graph()
+    assert _rows_equal(deg, adj, og.deg, og.adj) == []
+
+
+def test_float_rows_stand_the_tensor_core_pass_down(vann_mod):
+    """Rows that are not integers in [0, 255] set the inexact flag: the uint8 copy
+    still serves searches, but every prune runs on the CUDA cores."""
+    base = workload.mixture(2000, 128, 20, seed=46, sigma=0.05, integer=False, unit_norm=True)
+    idx = _build(vann_mod, base, 32, 64, ("f32", "u8"))
+    ref = _build(vann_mod, base, 32, 64, ("f32",))
+    info = idx.info()
+    assert info["pruned_tc"] == 0 and info["pruned_cuda"] > 0
+    _, da, aa = idx.get_graph()
+    _, db, ab = ref.get_graph()
+    assert _rows_equal(da, aa, db, ab) == []
+
+
+def test_consolidate_equals_cuda_core_path(vann_mod):
+    import torch
+
+    base = workload.mixture(5000, 128, 30, seed=47)
+    tc = _build(vann_mod, base, 32, 64, ("f32", "u8"), seed=5)
+    cc = _build(vann_mod, base, 32, 64, ("f32",), seed=5)
+    dead = np.random.default_rng(2).choice(5000, 600, replace=False).astype(np.int32)
+    extra = workload.mixture(300, 128, 30, seed=48)
+    for idx in (tc, cc):
+        idx.delete(torch.from_numpy(dead).cuda())
+        idx.consolidate()
+        idx.insert(torch.from_numpy(extra).cuda())
+    assert tc.info()["entry"] == cc.info()["entry"]
+    _, da, aa = tc.get_graph()
+    _, db, ab = cc.get_graph()
+    assert _rows_equal(da, aa, db, ab) == []
