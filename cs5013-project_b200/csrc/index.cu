@@ -195,8 +195,8 @@ struct vann_index {
             pa.gate     = u8_inexact();
             pa.in_list  = ovf.as<uint32_t>();
             pa.in_count = status + vann::kWordOverflow;
-            uint32_t* tc_counters = next_counter(st);  // [0] first pass, [1] second pass
-            VCHECK(cudaMemsetAsync(tc_counters + 1, 0, sizeof(uint32_t), st));
+            uint32_t* tc_counters = next_counter(st);  // one per pass
+            VCHECK(cudaMemsetAsync(tc_counters + 1, 0, 2 * sizeof(uint32_t), st));
             VCHECK(vann::launch_prune_tc(pa, ovf.as<uint32_t>() + pa.n_nodes, tc_counters, num_sms, st));
             pa.counter = next_counter(st);
         }

@@ -88,7 +88,7 @@ struct PruneArgs {
 // is set, else only the in_list slots the tensor-core passes handed over.
 cudaError_t launch_prune(const PruneArgs& a, int num_sms, cudaStream_t st);
 bool        prune_tc_supported(uint32_t D, uint32_t R);
-// ws: 2 * n_nodes + 4 words of scratch; counters: two zeroed work counters
+// ws: 2 * n_nodes + 4 words of scratch; counters: three zeroed work counters
 cudaError_t launch_prune_tc(const PruneArgs& a, uint32_t* ws, uint32_t* counters, int num_sms, cudaStream_t st);
 
 // graph utilities (graph_ops.cu)

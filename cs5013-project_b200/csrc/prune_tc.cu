@@ -112,7 +112,7 @@ __device__ __forceinline__ uint32_t dp4a_u(uint32_t a, uint32_t b, uint32_t c) {
 
 // shared memory of one CTA handling up to maxc candidates per node
 struct TcLayout {
-    uint32_t rows, nodev, cid, cd, keys, perm, sid, sd, nrm, pm, bar, misc, bytes;
+    uint32_t rows, nodev, cid, cd, keys, perm, sid, sd, nrm, pm, bmask, bar, misc, bytes;
     __host__ __device__ static TcLayout make(uint32_t D, uint32_t maxc) {
         TcLayout l;
         l.rows  = 0;                  // maxc x D bytes, canonical layout, sorted order
@@ -125,9 +125,10 @@ struct TcLayout {
         l.sd    = l.sid + 4 * maxc;
         l.nrm   = l.sd + 4 * maxc;
         l.pm    = l.nrm + 4 * maxc;   // [maxc][maxc / 32] prune masks
-        l.bar   = l.pm + maxc * maxc / 8;
+        l.bmask = l.pm + maxc * maxc / 8;  // sorted positions holding B candidates
+        l.bar   = l.bmask + maxc / 8;
         l.misc  = l.bar + 8;
-        l.bytes = l.misc + 4 * 8;
+        l.bytes = l.misc + 4 * 16;
         return l;
     }
 };
@@ -161,7 +162,8 @@ __global__ void __launch_bounds__(kThreads) prune_tc_kernel(PruneArgs a, uint32_
     float*         sd    = reinterpret_cast<float*>(smem + lay.sd);
     uint32_t*      nrm   = reinterpret_cast<uint32_t*>(smem + lay.nrm);
     uint32_t*      pm    = reinterpret_cast<uint32_t*>(smem + lay.pm);
-    uint32_t*      misc  = reinterpret_cast<uint32_t*>(smem + lay.misc);  // [0] tmem, [2..3] node slot
+    uint32_t*      bmask = reinterpret_cast<uint32_t*>(smem + lay.bmask);
+    uint32_t*      misc  = reinterpret_cast<uint32_t*>(smem + lay.misc);  // [0] tmem, [2..13] work items
     const uint32_t bar    = saddr(smem + lay.bar);
     const uint32_t rows_s = saddr(rows);
 
@@ -187,28 +189,45 @@ __global__ void __launch_bounds__(kThreads) prune_tc_kernel(PruneArgs a, uint32_
     bool           failed = false;
     uint32_t       done   = 0;  // nodes pruned by this CTA
 
-    for (uint32_t it = 0;; ++it) {
-        uint32_t* slot = misc + 2 + (it & 1u);
-        if (tid == 0) {
-            const uint32_t i = atomicAdd(counter, 1u);
-            *slot            = i < nwork ? (in_list ? __ldg(in_list + i) : i) : kNone;
+    // The next work item (slot, node, |A|, A offset, |B|) is fetched by one thread
+    // while the CTA prunes the current one, so its chain of dependent loads (work
+    // counter, node id, list bounds, degree) is off the critical path.
+    auto fetch = [&](uint32_t* item) {
+        uint32_t       w = kNone, node = kNone, nA = 0, aoff = 0, nB = 0;
+        const uint32_t i = atomicAdd(counter, 1u);
+        if (i < nwork) {
+            w    = in_list ? __ldg(in_list + i) : i;
+            node = a.node_ids ? __ldg(a.node_ids + w) : w;  // kNone: the padded slots' run
+            if (node != kNone) {
+                if (rev) {
+                    const uint32_t ci = a.csr_by_slot ? w : node;
+                    nA                = __ldg(a.csr_cnt + ci);
+                    aoff              = __ldg(a.csr_off + ci);
+                    if (a.skip_empty && nA == 0u) node = kNone;
+                    nA = min(nA, a.cap);
+                } else {
+                    nA = min(__ldg(a.a_n + w), a.a_stride);
+                }
+                if (node != kNone && a.use_b) nB = min(a.deg[node], R);
+            }
         }
-        __syncthreads();
-        const uint32_t w = *slot;
+        item[0] = w;
+        item[1] = node;
+        item[2] = nA;
+        item[3] = aoff;
+        item[4] = nB;
+    };
+    if (tid == 32) fetch(misc + 2);
+    __syncthreads();
+
+    for (uint32_t it = 0;; ++it, __syncthreads()) {
+        const uint32_t* cur  = misc + 2 + 6 * (it & 1u);
+        const uint32_t  w    = cur[0];
+        const uint32_t  node = cur[1];
+        const uint32_t  nA = cur[2], aoff = cur[3], nB = cur[4];
         if (w == kNone) break;
-        const uint32_t node = a.node_ids ? __ldg(a.node_ids + w) : w;
-        if (node == kNone) continue;  // the padded slots' run in the sorted edge list
-        uint32_t nA = 0, aoff = 0;
-        if (rev) {
-            const uint32_t ci = a.csr_by_slot ? w : node;
-            nA   = __ldg(a.csr_cnt + ci);
-            aoff = __ldg(a.csr_off + ci);
-            if (a.skip_empty && nA == 0u) continue;
-            nA = min(nA, a.cap);
-        } else {
-            nA = min(__ldg(a.a_n + w), a.a_stride);
-        }
-        const uint32_t nB = a.use_b ? min(__ldg(a.deg + node), R) : 0u;
+        if (tid == 32) fetch(misc + 2 + 6 * ((it + 1u) & 1u));
+        if (node == kNone) continue;
         const uint32_t nc = nA + nB;
         if (nc > MAXC) {
             if (tid == 0) out_list[atomicAdd(out_count, 1u)] = w;
@@ -290,10 +309,18 @@ __global__ void __launch_bounds__(kThreads) prune_tc_kernel(PruneArgs a, uint32_
 
         // --- 4. the first ncap candidates in sorted order: rows staged for the MMA
         const uint32_t m = min(nc, a.cap);
-        for (uint32_t t = tid; t < m; t += kThreads) {
-            const uint32_t i = perm[t];
-            sid[t]           = cid[i];
-            sd[t]            = cd[i];
+#pragma unroll
+        for (uint32_t q = 0; q < NB; ++q) {
+            const uint32_t t = 128u * q + tid;
+            bool           b = false;
+            if (t < m) {
+                const uint32_t i = perm[t];
+                sid[t]           = cid[i];
+                sd[t]            = cd[i];
+                b                = i >= nA;
+            }
+            const uint32_t bits = __ballot_sync(0xffffffffu, b);
+            if (lane == 0) bmask[4u * q + warp] = bits;
         }
         for (uint32_t x = tid; x < m * nchunk; x += kThreads) {
             const uint32_t t = x / nchunk, c = x - t * nchunk;
@@ -394,22 +421,79 @@ __global__ void __launch_bounds__(kThreads) prune_tc_kernel(PruneArgs a, uint32_
                 const uint32_t left = m - 32u * lane;
                 live                = left >= 32u ? ~0u : (1u << left) - 1u;
             }
-            uint32_t ndeg = 0;
-            while (ndeg < R) {
-                const uint32_t bm = __ballot_sync(0xffffffffu, live != 0u);
-                if (bm == 0u) break;
-                const uint32_t k0 = __ffs(bm) - 1u;
-                const uint32_t wv = __shfl_sync(0xffffffffu, live, k0);
-                const uint32_t t  = 32u * k0 + __ffs(wv) - 1u;
-                if (lane == 0) {
-                    const uint32_t id               = sid[t];
-                    a.adj[(uint64_t)node * R + ndeg]   = id;
-                    a.adj_h[(uint64_t)node * R + ndeg] = bloom_pack(id);
+            uint64_t       out  = (uint64_t)node * R;
+            uint32_t       ndeg = 0;
+            auto emit = [&](uint32_t t, uint32_t slot) {
+                const uint32_t id = sid[t];
+                a.adj[out + slot]   = id;
+                a.adj_h[out + slot] = bloom_pack(id);
+            };
+            if (!a.consistent) {
+                // one round per chosen neighbour
+                while (ndeg < R) {
+                    const uint32_t bm = __ballot_sync(0xffffffffu, live != 0u);
+                    if (bm == 0u) break;
+                    const uint32_t k0 = __ffs(bm) - 1u;
+                    const uint32_t wv = __shfl_sync(0xffffffffu, live, k0);
+                    const uint32_t t  = 32u * k0 + __ffs(wv) - 1u;
+                    if (lane == 0) emit(t, ndeg);
+                    ++ndeg;
+                    if (ndeg >= R) break;
+                    if (lane < QW) live &= ~pm[t * QW + lane];
+                    if (lane == k0) live &= ~(1u << (t & 31u));
                 }
-                ++ndeg;
-                if (ndeg >= R) break;
-                if (lane < QW) live &= ~pm[t * QW + lane];
-                if (lane == k0) live &= ~(1u << (t & 31u));
+            } else {
+                // B came out of RobustPrune with this alpha, so no B candidate prunes
+                // another: every live B candidate before the next live A candidate is
+                // chosen in one step, then that A candidate is decided.
+                const uint32_t bw = lane < QW ? bmask[lane] : 0u;
+                while (ndeg < R) {
+                    const uint32_t aw  = live & ~bw;
+                    const uint32_t bmA = __ballot_sync(0xffffffffu, aw != 0u);
+                    uint32_t       tA  = m;
+                    if (bmA) {
+                        const uint32_t k = __ffs(bmA) - 1u;
+                        tA               = 32u * k + __ffs(__shfl_sync(0xffffffffu, aw, k)) - 1u;
+                    }
+                    uint32_t run = 0u;
+                    if (lane < QW) {
+                        const uint32_t lo     = 32u * lane;
+                        const uint32_t before = tA >= lo + 32u ? ~0u : (tA <= lo ? 0u : (1u << (tA - lo)) - 1u);
+                        run                   = live & bw & before;
+                    }
+                    const uint32_t cnt = __popc(run);
+                    uint32_t       inc = cnt;  // inclusive prefix over lanes
+#pragma unroll
+                    for (uint32_t o = 1; o < 32; o <<= 1) {
+                        const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+                        if (lane >= o) inc += v;
+                    }
+                    const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+                    const uint32_t take  = min(total, R - ndeg);
+                    uint32_t       j     = inc - cnt;
+                    for (uint32_t bits = run; bits != 0u && j < take; bits &= bits - 1u, ++j)
+                        emit(32u * lane + __ffs(bits) - 1u, ndeg + j);
+                    ndeg += take;
+                    if (ndeg >= R) break;
+                    live &= ~run;
+                    uint32_t acc = 0u;  // everything the run prunes
+                    for (uint32_t q = 0; q < QW; ++q) {
+                        for (uint32_t rq = __shfl_sync(0xffffffffu, run, q); rq != 0u; rq &= rq - 1u) {
+                            const uint32_t t = 32u * q + __ffs(rq) - 1u;
+                            if (lane < QW) acc |= pm[t * QW + lane];
+                        }
+                    }
+                    live &= ~acc;
+                    if (tA >= m) break;  // every live candidate was in the run
+                    const uint32_t tw = __shfl_sync(0xffffffffu, live, tA >> 5);
+                    if ((tw >> (tA & 31u)) & 1u) {
+                        if (lane == 0) emit(tA, ndeg);
+                        ++ndeg;
+                        if (ndeg >= R) break;
+                        if (lane < QW) live &= ~pm[tA * QW + lane];
+                        if (lane == (tA >> 5)) live &= ~(1u << (tA & 31u));
+                    }
+                }
             }
             if (lane == 0) a.deg[node] = ndeg;
         }
@@ -467,22 +551,33 @@ cudaError_t launch_tc(const PruneArgs& a, uint32_t* counter, const uint32_t* in_
 
 }  // namespace
 
-// Two passes: up to 256 candidates (4 CTAs per SM), then the nodes it handed over
-// with up to 512 (2 CTAs per SM); larger ones are left in a.in_list for prune_kernel.
-// ws: 2 * n_nodes + 4 words of device scratch, counters: two zeroed work counters.
+// Passes of 256 candidates (4 CTAs per SM), then 512 (2 per SM), then 768 (one per
+// SM, when its shared memory fits: D <= 128) for the nodes each pass handed over;
+// larger ones are left in a.in_list for prune_kernel.
+// ws: 2 * n_nodes + 4 words of device scratch; counters: three zeroed work counters.
 cudaError_t launch_prune_tc(const PruneArgs& a, uint32_t* ws, uint32_t* counters, int num_sms, cudaStream_t st) {
     if (a.n_nodes == 0) return cudaSuccess;
     if (!prune_tc_supported(a.D, a.R) || !a.vecs_u8 || !a.gate || !a.in_list || !a.in_count)
         return cudaErrorInvalidValue;
-    uint32_t* list1  = ws;
-    uint32_t* count1 = ws + a.n_nodes;
-    cudaError_t e = cudaMemsetAsync(count1, 0, sizeof(uint32_t), st);
+    int dev = 0, max_optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(a.in_count, 0, sizeof(uint32_t), st);
+    e = cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
+    const bool third  = TcLayout::make(a.D, 768).bytes <= (uint32_t)max_optin;
+    uint32_t*  list1  = ws;
+    uint32_t*  count1 = ws + a.n_nodes;
+    uint32_t*  list2  = third ? ws + a.n_nodes + 1 : a.in_list;
+    uint32_t*  count2 = third ? ws + 2 * a.n_nodes + 1 : a.in_count;
+    for (uint32_t* c : {count1, count2, a.in_count}) {
+        e = cudaMemsetAsync(c, 0, sizeof(uint32_t), st);
+        if (e != cudaSuccess) return e;
+    }
     e = launch_tc<256>(a, counters, nullptr, nullptr, list1, count1, a.n_nodes, num_sms, st);
     if (e != cudaSuccess) return e;
-    return launch_tc<512>(a, counters + 1, list1, count1, a.in_list, a.in_count, a.n_nodes, num_sms, st);
+    e = launch_tc<512>(a, counters + 1, list1, count1, list2, count2, a.n_nodes, num_sms, st);
+    if (e != cudaSuccess || !third) return e;
+    return launch_tc<768>(a, counters + 2, list2, count2, a.in_list, a.in_count, a.n_nodes, num_sms, st);
 }
 
 }  // namespace vann

@@ -69,11 +69,11 @@ def test_loaded_start_graph_two_tiles(oracle, vann_mod):
     assert _rows_equal(gdeg, gadj, og.deg, og.adj) == []
 
 
-@pytest.mark.parametrize("L,max_visited,cuda_share", [(300, 600, False), (600, 800, True)])
+@pytest.mark.parametrize("L,max_visited,cuda_share", [(300, 600, False), (600, 800, False), (900, 1100, True)])
 def test_large_candidate_lists(oracle, vann_mod, L, max_visited, cuda_share):
     """257..512 candidates (expansion lists at L=300) take the second tensor-core
-    pass; more than 512 (L=600) are handed to the CUDA-core kernel.  Either way the
-    graph is the oracle's."""
+    pass, up to 768 (L=600) the third; more (L=900) are handed to the CUDA-core
+    kernel.  Every way the graph is the oracle's."""
     import torch
 
     base = workload.mixture(2500, 128, 20, seed=45)
