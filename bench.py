@@ -496,7 +496,8 @@ def main_churn():
     cap = int(n * 1.1)
     vec_by_id = torch.zeros((cap, DIM), dtype=torch.float32, device=dev)
     vec_by_id[:n] = torch.from_numpy(base).to(dev)
-    idx = vann.Index(DIM, R, L_BUILD, ALPHA, capacity=cap)
+    # integer rows: the exact uint8 copy lets RobustPrune run on the tensor cores
+    idx = vann.Index(DIM, R, L_BUILD, ALPHA, capacity=cap, stores=("f32", "u8"))
     t0 = time.time()
     idx.build(vec_by_id[:n].contiguous(), batch=BATCH, seed=2024)
     torch.cuda.synchronize()
@@ -548,6 +549,7 @@ def main_churn():
             "min_recall@10": min(o["recall@10_L100"] for o in out) if out else None,
             "median_inserts_per_s": float(np.median([o["inserts_per_s"] for o in out])) if out else None,
             "median_deletes_per_s": float(np.median([o["deletes_per_s"] for o in out])) if out else None,
+            "prunes": {k: idx.info()[k] for k in ("pruned_tc", "pruned_cuda")},
             "rounds": out}
     print(json.dumps(line), flush=True)
     return 0
