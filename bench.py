@@ -56,9 +56,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile", action="store_true", help="short run for a profiler capture")
-    ap.add_argument("--config", default="search", choices=["search", "churn", "precision", "serve"],
-                    help="search: the headline line; churn / precision: the FreshVamana churn and "
-                         "reduced-precision configurations (their own JSON lines)")
+    ap.add_argument("--config", default="search", choices=["search", "churn", "precision", "serve", "build"],
+                    help="search: the headline line; churn / precision / serve: configurations 3-5; "
+                         "build: index build and insert throughput (their own JSON lines)")
     ap.add_argument("--rounds", type=int, default=20)
     ap.add_argument("--rate", type=float, default=50_000.0, help="serve: offered requests/s")
     ap.add_argument("--duration", type=float, default=5.0, help="serve: seconds of arrivals")
@@ -276,7 +276,7 @@ def main():
     traffic = None
     try:
         prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
-        tkey = f"search_kernel_rw<StoreU8,0,2,1,6> {n}x{DIM} nq={nq} L={hr['L']} k={K}"
+        tkey = f"search_kernel_rw<StoreU8> {n}x{DIM} nq={nq} L={hr['L']} k={K}"
         if head == "u8" and tkey in prof:
             traffic = prof[tkey]["dram_bytes_read"] + prof[tkey]["dram_bytes_write"]
     except (OSError, KeyError, ValueError):
@@ -728,6 +728,53 @@ def main_serve():
     return 0
 
 
+def main_build():
+    """Index build and insert throughput: --n rows (default 1M) x 128, integer-valued, 1,000
+    clusters, R=64 L=100 alpha=1.2, built in batches of 10,000 with the exact uint8 copy
+    (RobustPrune on the tensor cores), then single-call inserts of 1 .. 10,000 new rows,
+    three of each size, timed by CUDA events around each call."""
+    args = parse()
+    import torch
+
+    import vann
+    from vann import workload
+
+    dev = torch.device("cuda", 0)
+    n = args.n
+    sizes = [1, 10, 100, 1000, 10000]
+    base = workload.mixture(n, DIM, 1000, seed=1)
+    base_d = torch.from_numpy(base).to(dev)
+    idx = vann.Index(DIM, R, L_BUILD, ALPHA, capacity=n + 3 * sum(sizes), stores=("f32", "u8"))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    idx.build(base_d, batch=BATCH, seed=2024)
+    e1.record()
+    torch.cuda.synchronize()
+    build_ms = e0.elapsed_time(e1)
+    info = idx.info()
+    inserts = {}
+    for m in sizes:
+        extra = torch.from_numpy(workload.mixture(m, DIM, 1000, seed=100 + m)).to(dev)
+        ts = []
+        for _ in range(3):
+            e0.record()
+            idx.insert(extra)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        inserts[str(m)] = {"ms": round(float(np.median(ts)), 3), "rows_per_s": round(m / (np.median(ts) / 1e3), 1)}
+    line = {"metric": "index build and insert throughput",
+            "config": {"workload": f"{n}x{DIM} integer-valued f32, 1000-cluster mixture; R={R} L={L_BUILD} "
+                                   f"alpha={ALPHA}; batches of {BATCH}; stores f32+u8"},
+            "data": "synthetic (seeded clipped Gaussian mixture)",
+            "build_s": round(build_ms / 1e3, 3), "build_rows_per_s": round(n / (build_ms / 1e3), 1),
+            "prunes": {k: info[k] for k in ("pruned_tc", "pruned_cuda")},
+            "insert_median_of_3": inserts}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 if __name__ == "__main__":
     if "--impl" in sys.argv and sys.argv[sys.argv.index("--impl") + 1] == "reference":
         sys.exit(main_reference())
@@ -739,4 +786,6 @@ if __name__ == "__main__":
             sys.exit(main_precision())
         if cfg == "serve":
             sys.exit(main_serve())
+        if cfg == "build":
+            sys.exit(main_build())
     sys.exit(main())

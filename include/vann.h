@@ -187,9 +187,10 @@ vann_status vann_consolidate(vann_index* index, void* stream);
  * index.  Requests carry host data.  Searches queued while batch slots are busy
  * are admitted together into the next free slot as one uneven launch (own k
  * and L per request) with its copies on the slot's stream, so several batches
- * run at once (continuous batching).  Writes keep their place in the request
- * order: each search sees exactly the writes submitted before it.  Slot device
- * memory is allocated at creation and capped by hbm_budget. */
+ * run at once (continuous batching).  By default writes keep their place in the
+ * request order: each search sees exactly the writes submitted before it.  With
+ * commit_interval_us > 0 writes are group-committed instead (see the field).  Slot
+ * device memory is allocated at creation and capped by hbm_budget. */
 typedef struct {
     uint32_t max_batch;   /* queries per admitted batch */
     uint32_t slots;       /* batches on the GPU at once (one stream each) */
