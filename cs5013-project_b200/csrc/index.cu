@@ -127,6 +127,7 @@ struct vann_index {
     size_t    held     = 0;
 
     std::vector<uint32_t> free_ids;  // consolidated ids, reused by inserts
+    uint64_t stage_n = 0;  // rows in the insert list (stage), outside the graph
     // per-query L / k arrays of the vann_search_uneven call in progress
     const uint32_t* pending_Lq = nullptr;
     const uint32_t* pending_kq = nullptr;
@@ -138,7 +139,7 @@ struct vann_index {
         return it == tuned.end() ? 0 : it->second;
     }
 
-    DevBuf vis_ids, vis_d, vis_n, nodes, runs, ovf, e_keys, e_vals, e_keys2, e_vals2, counts, offsets, cub_tmp,
+    DevBuf vis_ids, vis_d, vis_n, nodes, runs, ovf, stage, s2_ids, s2_d, e_keys, e_vals, e_keys2, e_vals2, counts, offsets, cub_tmp,
         medoid_ws, gather, cand, cand_n, cand_d, list_n, out_tmp;
 
     void alloc(void** ptr, size_t bytes) {
@@ -155,7 +156,7 @@ struct vann_index {
         cudaFree(tomb);
         cudaFree(counters);
         cudaFree(status);
-        for (DevBuf* b : {&vis_ids, &vis_d, &vis_n, &nodes, &runs, &ovf, &e_keys, &e_vals, &e_keys2, &e_vals2,
+        for (DevBuf* b : {&vis_ids, &vis_d, &vis_n, &nodes, &runs, &ovf, &stage, &s2_ids, &s2_d, &e_keys, &e_vals, &e_keys2, &e_vals2,
                           &counts, &offsets, &cub_tmp, &medoid_ws, &gather, &cand, &cand_n, &cand_d,
                           &list_n, &out_tmp})
             b->release();
@@ -493,6 +494,7 @@ vann_status vann_get_info(const vann_index* h, vann_info* out) {
         VCHECK(cudaMemcpy(pr, h->status + vann::kWordPruned, sizeof(pr), cudaMemcpyDeviceToHost));
         out->pruned_tc   = pr[0];
         out->pruned_cuda = pr[1];
+        out->staged      = h->stage_n;
     });
 }
 
@@ -685,6 +687,77 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
 }
 
 int vann_search_variant_count(void) { return vann::search_variants(); }
+
+vann_status vann_stage_insert(vann_index* h, const float* d_vecs, uint64_t n, void* stream) {
+    return guard([&] {
+        VREQUIRE(h && (d_vecs || n == 0), VANN_ERR_INVALID, "null argument");
+        if (n == 0) return;
+        cudaStream_t st  = S(stream);
+        const size_t row = sizeof(float) * h->p.dim;
+        if ((h->stage_n + n) * row > h->stage.bytes) {  // grow by 1.5x, keeping the rows
+            const size_t nb = std::max((h->stage_n + n) * row, h->stage.bytes * 3 / 2);
+            void*        np = nullptr;
+            VCHECK(cudaMalloc(&np, nb));
+            cudaError_t e = h->stage_n ? cudaMemcpyAsync(np, h->stage.p, h->stage_n * row,
+                                                         cudaMemcpyDeviceToDevice, st)
+                                       : cudaSuccess;
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) {
+                cudaFree(np);
+                VCHECK(e);
+            }
+            h->stage.release();
+            h->stage.p     = np;
+            h->stage.bytes = nb;
+        }
+        VCHECK(cudaMemcpyAsync(static_cast<char*>(h->stage.p) + h->stage_n * row, d_vecs, n * row,
+                               cudaMemcpyDeviceToDevice, st));
+        VCHECK(cudaStreamSynchronize(st));
+        h->stage_n += n;
+    });
+}
+
+vann_status vann_search_staged(vann_index* h, const float* d_queries, uint64_t nq, const vann_search_params* sp,
+                               uint32_t* d_ids, float* d_dists, float* d_vecs_out, void* stream) {
+    vann_status st_search = VANN_OK;
+    vann_status s         = guard([&] {
+        VREQUIRE(h && sp && (nq == 0 || (d_queries && d_ids && d_dists)), VANN_ERR_INVALID, "null argument");
+        VREQUIRE(sp->L >= 1 && sp->L <= 1024, VANN_ERR_INVALID, "need 1 <= L <= 1024");
+        if (nq == 0) return;
+        cudaStream_t       st = S(stream);
+        vann_search_params p  = *sp;
+        p.k                   = p.L;  // the whole worklist, in its order
+        h->s2_ids.ensure(sizeof(uint32_t) * nq * p.L);
+        h->s2_d.ensure(sizeof(float) * nq * p.L);
+        st_search = vann_search(h, d_queries, nq, &p, h->s2_ids.as<uint32_t>(), h->s2_d.as<float>(), stream);
+        if (st_search != VANN_OK) return;
+        vann::StagedArgs a{};
+        a.queries   = d_queries;
+        a.nq        = nq;
+        a.vecs      = h->vecs;
+        a.graph_ids = h->s2_ids.as<uint32_t>();
+        a.L         = p.L;
+        a.D         = h->p.dim;
+        a.stage     = h->stage.as<float>();
+        a.n_stage   = h->stage_n;
+        a.out_ids   = d_ids;
+        a.out_d     = d_dists;
+        a.out_vecs  = d_vecs_out;
+        VCHECK(vann::launch_staged_merge(a, h->num_sms, st));
+    });
+    return s != VANN_OK ? s : st_search;
+}
+
+vann_status vann_patch_graph(vann_index* h, uint32_t* d_ids_out, void* stream) {
+    vann_status st_insert = VANN_OK;
+    vann_status s         = guard([&] {
+        VREQUIRE(h, VANN_ERR_INVALID, "null argument");
+        if (h->stage_n == 0) return;
+        st_insert = vann_insert(h, h->stage.as<float>(), h->stage_n, d_ids_out, stream);
+        if (st_insert == VANN_OK) h->stage_n = 0;
+    });
+    return s != VANN_OK ? s : st_insert;
+}
 
 vann_status vann_autotune(vann_index* h, const float* d_queries, uint64_t nq, const vann_search_params* sp,
                           float* h_ms_out, void* stream) {

@@ -91,6 +91,22 @@ bool        prune_tc_supported(uint32_t D, uint32_t R);
 // ws: 2 * n_nodes + 4 words of scratch; counters: three zeroed work counters
 cudaError_t launch_prune_tc(const PruneArgs& a, uint32_t* ws, uint32_t* counters, int num_sms, cudaStream_t st);
 
+// searchPoints2's merge of graph results with the insert list (staged.cu)
+struct StagedArgs {
+    const float*    queries;    // nq x D
+    uint64_t        nq;
+    const float*    vecs;       // graph rows
+    const uint32_t* graph_ids;  // nq x L worklist entries (kNone: padding)
+    uint32_t        L, D;
+    const float*    stage;      // n_stage x D insert-list rows
+    uint64_t        n_stage;
+    uint32_t*       out_ids;    // nq x L: graph id, or 0x80000000 | insert-list row
+    float*          out_d;      // nq x L
+    float*          out_vecs;   // nq x L x D or null
+    uint32_t        p2;         // set by the launcher
+};
+cudaError_t launch_staged_merge(const StagedArgs& a, int num_sms, cudaStream_t st);
+
 // graph utilities (graph_ops.cu)
 cudaError_t launch_random_graph(uint32_t* deg, uint32_t* adj, uint32_t* adj_h, uint64_t first,
                                 uint64_t n, uint32_t R, uint64_t seed, cudaStream_t st);

@@ -25,6 +25,7 @@ STORE_F32, STORE_BF16, STORE_FP8, STORE_U8 = 0, 1, 2, 3
 STORES = {"f32": STORE_F32, "bf16": STORE_BF16, "fp8": STORE_FP8, "u8": STORE_U8}
 QUIRK_SKIP_BATCH_INDEX = 0x1
 NONE_ID = 0xFFFFFFFF
+STAGED_BIT = 0x80000000  # VANN_STAGED_ID(s): insert-list row s in vann_search_staged results
 
 # every symbol include/vann.h declares
 EXPORTS = [
@@ -34,6 +35,7 @@ EXPORTS = [
     "vann_consolidate", "vann_medoid_noalloc", "vann_server_create", "vann_server_destroy",
     "vann_server_submit_search", "vann_server_submit_insert", "vann_server_submit_delete",
     "vann_server_submit_consolidate", "vann_server_wait", "vann_server_get_stats",
+    "vann_stage_insert", "vann_search_staged", "vann_patch_graph",
 ]
 
 
@@ -58,7 +60,7 @@ class Info(C.Structure):
     _fields_ = [("size", C.c_uint64), ("capacity", C.c_uint64), ("live", C.c_uint64),
                 ("free_ids", C.c_uint64), ("entry", C.c_uint32), ("dim", C.c_uint32),
                 ("degree", C.c_uint32), ("consistent", C.c_uint32), ("device_bytes", C.c_uint64),
-                ("pruned_tc", C.c_uint64), ("pruned_cuda", C.c_uint64)]
+                ("pruned_tc", C.c_uint64), ("pruned_cuda", C.c_uint64), ("staged", C.c_uint64)]
 
 
 class ServerParams(C.Structure):
@@ -116,6 +118,9 @@ def lib():
             "vann_server_submit_consolidate": (C.c_int, [vp, C.POINTER(u64)]),
             "vann_server_wait": (C.c_int, [vp, u64, vp, vp, C.POINTER(C.c_double), C.POINTER(u64), u32]),
             "vann_server_get_stats": (C.c_int, [vp, C.POINTER(ServerStats)]),
+            "vann_stage_insert": (C.c_int, [vp, vp, u64, vp]),
+            "vann_search_staged": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp, vp, vp]),
+            "vann_patch_graph": (C.c_int, [vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -296,6 +301,34 @@ class Index:
     def consolidate(self, stream=None):
         _check(lib().vann_consolidate(self._h, _stream_ptr(stream)))
 
+    def stage_insert(self, vecs, stream=None):
+        """Append rows to the insert list, outside the graph (vann_stage_insert)."""
+        torch = _torch()
+        _check(lib().vann_stage_insert(self._h, _dev(vecs, torch.float32), vecs.shape[0], _stream_ptr(stream)))
+
+    def search_staged(self, queries, L: int, store: str = "f32", rerank: bool = False, quirks: int = 0,
+                      with_vecs: bool = False, stream=None):
+        """searchPoints2 (vann_search_staged): n x L graph ids or STAGED_BIT | row, distances,
+        and with_vecs the n x L x dim rows."""
+        torch = _torch()
+        n = queries.shape[0]
+        sp = SearchParams(L, L, STORES[store], int(rerank), quirks, 0)
+        ids = torch.empty((n, L), dtype=torch.int32, device=queries.device)
+        d = torch.empty((n, L), dtype=torch.float32, device=queries.device)
+        v = torch.empty((n, L, queries.shape[1]), dtype=torch.float32, device=queries.device) if with_vecs else None
+        _check(lib().vann_search_staged(self._h, _dev(queries, torch.float32), n, C.byref(sp),
+                                        _dev(ids, torch.int32), _dev(d, torch.float32),
+                                        _dev(v, torch.float32) if v is not None else None, _stream_ptr(stream)))
+        return (ids, d, v) if with_vecs else (ids, d)
+
+    def patch_graph(self, stream=None):
+        """Move the insert list into the graph (vann_patch_graph); returns the new ids."""
+        torch = _torch()
+        n = self.info()["staged"]
+        ids = torch.empty(n, dtype=torch.int32, device="cuda")
+        _check(lib().vann_patch_graph(self._h, _dev(ids, torch.int32) if n else None, _stream_ptr(stream)))
+        return ids
+
 
 class Server:
     """Continuous-batching request loop over one Index (vann_server_*).  Requests
@@ -382,10 +415,11 @@ class Vamana:
     """The reference's index class (vamana/include/vamana.cuh:36-146) on top of Index.
 
     ``Vamana(vecs, R, L, alpha, ...)`` builds like the reference constructor
-    (vamana_impl.cuh:10-20 -> runVamana :289-360).  insertPoints stages vectors
-    like the reference's InsertList (vamana_impl.cuh:22-33); patchGraph inserts
-    the staged batch and consolidates deletes (:182-265); deletePoints matches
-    by vector (:35-53); searchPoints returns the n x L worklist ids (:55-96).
+    (vamana_impl.cuh:10-20 -> runVamana :289-360).  insertPoints appends to the
+    index's insert list (vamana_impl.cuh:22-33); searchPoints2 merges graph results
+    with it and returns the n x L x dim rows (:98-180); patchGraph inserts the list
+    and consolidates deletes (:182-265); deletePoints matches by vector (:35-53);
+    searchPoints returns the n x L worklist ids (:55-96).
     """
 
     def __init__(self, vecs, R: int = 64, L: int = 199, alpha: float = 1.5, capacity: int | None = None,
@@ -397,10 +431,9 @@ class Vamana:
         self.index = Index(vecs.shape[1], R, L, alpha, capacity or max(int(n * 1.3), n + 1), max_visited,
                            max_reverse, self.quirks)
         self.index.build(vecs, batch=0, seed=seed, entry=entry)
-        self._staged = []
 
     def insertPoints(self, d_vecs, num: int | None = None):
-        self._staged.append(d_vecs[: num if num is not None else d_vecs.shape[0]].contiguous())
+        self.index.stage_insert(d_vecs[: num if num is not None else d_vecs.shape[0]].contiguous())
 
     def deletePoints(self, d_vecs, num: int | None = None):
         return self.index.delete_by_vector(d_vecs[: num if num is not None else d_vecs.shape[0]].contiguous())
@@ -410,11 +443,13 @@ class Vamana:
         ids, _ = self.index.search(q, k=self.L, L=self.L, quirks=self.quirks)
         return ids
 
+    def searchPoints2(self, d_q, num: int | None = None):
+        q = d_q[: num if num is not None else d_q.shape[0]].contiguous()
+        _, _, vecs = self.index.search_staged(q, L=self.L, quirks=self.quirks, with_vecs=True)
+        return vecs
+
     def patchGraph(self):
-        torch = _torch()
-        if self._staged:
-            self.index.insert(torch.cat(self._staged, 0).contiguous())
-            self._staged = []
+        self.index.patch_graph()
         self.index.consolidate()
 
     def saveGraph(self, path: str):

@@ -84,6 +84,7 @@ typedef struct {
     uint64_t device_bytes; /* device memory held by the index */
     uint64_t pruned_tc;    /* RobustPrune runs done with the Gram matrix on the tensor cores */
     uint64_t pruned_cuda;  /* RobustPrune runs done on the CUDA cores (float rows, overflow) */
+    uint64_t staged;       /* rows in the insert list (vann_stage_insert), not yet in the graph */
 } vann_info;
 
 typedef struct vann_index vann_index;
@@ -180,6 +181,32 @@ vann_status vann_delete_by_vector(vann_index* index, const float* d_vecs, uint64
  * re-pruned over its live out-neighbours plus the deleted nodes' live
  * out-neighbours; deleted ids are then freed for reuse.  Synchronises. */
 vann_status vann_consolidate(vann_index* index, void* stream);
+
+/* Vamana<T>::insertPoints (vamana_impl.cuh:22-33; InsertList::addVectors,
+ * insert_list.cuh:12-87): append n device rows (n x dim FP32) to the index's insert
+ * list, outside the graph.  vann_search_staged sees them; vann_patch_graph moves
+ * them into the graph.  Synchronises `stream`. */
+vann_status vann_stage_insert(vann_index* index, const float* d_vecs, uint64_t n, void* stream);
+
+/* Vamana<T>::searchPoints2 (vamana_impl.cuh:98-180, merge_and_rerank_kernel
+ * utils.cuh:199-285): GreedySearch with worklist sp->L (sp->k is ignored), then the
+ * L worklist entries followed by every insert-list row compete for L slots by FP32
+ * squared distance, computed sequentially over the dimensions like l2_distance_sq
+ * (utils.cuh:150-158).  A candidate enters when strictly closer than the farthest
+ * slot and replaces the first slot at that distance; the slots are returned in
+ * stable distance order.  Per query L entries: d_ids holds graph ids, or
+ * VANN_STAGED_ID(s) for insert-list row s (0xFFFFFFFF for an unfilled slot);
+ * d_dists the distances; d_vecs_out (may be NULL) the rows themselves (nq x L x dim),
+ * which is what searchPoints2 returns.  Asynchronous on `stream`. */
+#define VANN_STAGED_ID(s) (0x80000000u | (uint32_t)(s))
+vann_status vann_search_staged(vann_index* index, const float* d_queries, uint64_t nq,
+                               const vann_search_params* sp, uint32_t* d_ids, float* d_dists,
+                               float* d_vecs_out, void* stream);
+
+/* The insert half of Vamana<T>::patchGraph (vamana_impl.cuh:182-265): every
+ * insert-list row, in order, goes into the graph as one vann_insert batch and the
+ * list is emptied.  d_ids_out (may be NULL) receives their graph ids.  Synchronises. */
+vann_status vann_patch_graph(vann_index* index, uint32_t* d_ids_out, void* stream);
 
 /* ---------------------------------------------------------------- serving loop
  * No counterpart in the reference, whose driver issues one call at a time on the

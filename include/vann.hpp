@@ -3,10 +3,12 @@
 // Drop-in for callers of the reference's `template <typename T> class Vamana`
 // (vamana/include/vamana.cuh:36-146): same member names and argument meaning.
 //   Vamana(graph_path, ...)    initGraph + runVamana (vamana_impl.cuh:10-20, 289-360)
-//   insertPoints(d_vecs, n)    stage vectors, visible after patchGraph (vamana_impl.cuh:22-33)
+//   insertPoints(d_vecs, n)    append to the insert list, outside the graph (vamana_impl.cuh:22-33)
 //   deletePoints(d_vecs, n)    lazy delete by exact vector match (vamana_impl.cuh:35-53)
 //   searchPoints(d_q, n)       device n x L worklist ids, caller cudaFree()s (vamana_impl.cuh:55-96)
-//   patchGraph()               insert the staged batch, consolidate deletes (vamana_impl.cuh:182-265)
+//   searchPoints2(d_q, n)      graph results merged with the insert list; device n x L x D
+//                              rows, caller cudaFree()s (vamana_impl.cuh:98-180)
+//   patchGraph()               insert the insert list, consolidate deletes (vamana_impl.cuh:182-265)
 //   saveGraph(path)            772-byte records at D=128, R=64 (vamana.cu:1346-1362)
 // Error behaviour: the reference's gpuErrchk prints and exit()s (utils.cuh:68-78);
 // this mirror throws vann::Error carrying the status and message instead.
@@ -59,20 +61,12 @@ class Vamana {
         check(vann_build(h_, d_vecs, n, 0, p_.seed, 0xFFFFFFFFu, nullptr));
     }
     ~Vamana() {
-        for (float* s : staged_) cudaFree(s);
         if (h_) vann_destroy(h_);
     }
     Vamana(const Vamana&) = delete;
     Vamana& operator=(const Vamana&) = delete;
 
-    void insertPoints(T* d_query_vecs, size_t num) {
-        if (num == 0) return;
-        float* copy = nullptr;
-        if (cudaMalloc(&copy, sizeof(float) * num * p_.dim) != cudaSuccess) throw Error(VANN_ERR_OOM, "cudaMalloc");
-        cudaMemcpy(copy, d_query_vecs, sizeof(float) * num * p_.dim, cudaMemcpyDeviceToDevice);
-        staged_.push_back(copy);
-        staged_n_.push_back(num);
-    }
+    void insertPoints(T* d_query_vecs, size_t num) { check(vann_stage_insert(h_, d_query_vecs, num, nullptr)); }
 
     void deletePoints(T* d_query_vecs, size_t num) {
         if (num == 0) return;
@@ -96,13 +90,33 @@ class Vamana {
         return ids;
     }
 
-    void patchGraph() {
-        for (size_t i = 0; i < staged_.size(); ++i) {
-            check(vann_insert(h_, staged_[i], staged_n_[i], nullptr, nullptr));
-            cudaFree(staged_[i]);
+    // n x L x D rows on the device (the reference's searchPoints2 result); free with cudaFree.
+    [[nodiscard]] T* searchPoints2(T* d_query_vecs, size_t num) {
+        uint32_t* ids  = nullptr;
+        float*    d    = nullptr;
+        T*        rows = nullptr;
+        if (cudaMalloc(&ids, sizeof(uint32_t) * num * p_.L) != cudaSuccess ||
+            cudaMalloc(&d, sizeof(float) * num * p_.L) != cudaSuccess ||
+            cudaMalloc(&rows, sizeof(T) * num * p_.L * p_.dim) != cudaSuccess) {
+            cudaFree(ids);
+            cudaFree(d);
+            throw Error(VANN_ERR_OOM, "cudaMalloc");
         }
-        staged_.clear();
-        staged_n_.clear();
+        vann_search_params sp{p_.L, p_.L, VANN_STORE_F32, 0,
+                              p_.reference_quirks ? VANN_QUIRK_SKIP_BATCH_INDEX : 0u, 0};
+        vann_status s = vann_search_staged(h_, d_query_vecs, num, &sp, ids, d, rows, nullptr);
+        if (s == VANN_OK) s = vann_sync(h_, nullptr);
+        cudaFree(ids);
+        cudaFree(d);
+        if (s != VANN_OK) {
+            cudaFree(rows);
+            check(s);
+        }
+        return rows;
+    }
+
+    void patchGraph() {
+        check(vann_patch_graph(h_, nullptr, nullptr));
         check(vann_consolidate(h_, nullptr));
     }
 
@@ -125,10 +139,8 @@ class Vamana {
         check(vann_create(&vp, &h_));
     }
 
-    VamanaParams        p_;
-    vann_index*         h_ = nullptr;
-    std::vector<float*> staged_;
-    std::vector<size_t> staged_n_;
+    VamanaParams p_;
+    vann_index*  h_ = nullptr;
 };
 
 }  // namespace vann

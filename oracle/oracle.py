@@ -69,6 +69,9 @@ def lib():
         L.vo_bruteforce_knn.restype = None
         L.vo_bruteforce_knn.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, C.c_int,
                                         C.c_void_p, C.c_void_p, C.c_int]
+        L.vo_merge_rerank.restype = None
+        L.vo_merge_rerank.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_int,
+                                      C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
         _LIB = L
     return _LIB
 
@@ -169,6 +172,24 @@ def bruteforce_knn(base: np.ndarray, q: np.ndarray, k: int, threads: int = 0):
     ids = np.empty((q.shape[0], k), np.uint32)
     d = np.empty((q.shape[0], k), np.float64)
     lib().vo_bruteforce_knn(_p(base), base.shape[0], _p(q), q.shape[0], base.shape[1], k, _p(ids), _p(d), threads)
+    return ids, d
+
+
+STAGED = 0x80000000
+
+
+def merge_rerank(vecs: np.ndarray, q: np.ndarray, graph_ids: np.ndarray, insert_list: np.ndarray):
+    """searchPoints2's merge of the L graph results with the insert list
+    (utils.cuh:199-285): ids (insert-list row s as STAGED | s) and distances, n x L."""
+    vecs = np.ascontiguousarray(vecs, dtype=np.float32)
+    q = np.ascontiguousarray(q, dtype=np.float32)
+    gi = np.ascontiguousarray(graph_ids, dtype=np.uint32)
+    il = np.ascontiguousarray(insert_list, dtype=np.float32).reshape(-1, vecs.shape[1])
+    nq, L = gi.shape
+    ids = np.empty((nq, L), np.uint32)
+    d = np.empty((nq, L), np.float32)
+    lib().vo_merge_rerank(_p(vecs), vecs.shape[1], _p(q), nq, _p(gi), L, _p(il) if len(il) else None,
+                          len(il), _p(ids), _p(d))
     return ids, d
 
 

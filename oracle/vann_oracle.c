@@ -502,3 +502,65 @@ void vo_bruteforce_knn(const float* base, int64_t n, const float* q, int64_t nq,
         }
     }
 }
+
+/* l2_distance_sq (vamana/include/utils.cuh:150-158): sequential over the
+ * dimensions, `dist += diff * diff` -- which nvcc contracts to one fused
+ * multiply-add per dimension, so fmaf here. */
+static float vo_l2_seq(const float* a, const float* b, int dim) {
+    float d = 0.0f;
+    for (int i = 0; i < dim; ++i) {
+        const float diff = a[i] - b[i];
+        d                = fmaf(diff, diff, d);
+    }
+    return d;
+}
+
+void vo_merge_rerank(const float* vecs, int dim, const float* q, int64_t nq, const uint32_t* graph_ids,
+                     int L, const float* insert_list, int64_t n_il, uint32_t* out_ids, float* out_d) {
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t qi = 0; qi < nq; ++qi) {
+        const float* qv   = q + (size_t)qi * dim;
+        float*       sd   = out_d + (size_t)qi * L;
+        uint32_t*    sid  = out_ids + (size_t)qi * L;
+        for (int k = 0; k < L; ++k) {
+            sd[k]  = INFINITY;
+            sid[k] = 0xFFFFFFFFu;
+        }
+        for (int64_t c = 0; c < L + n_il; ++c) {
+            uint32_t     id;
+            const float* row;
+            if (c < L) {
+                id = graph_ids[(size_t)qi * L + c];
+                if (id == 0xFFFFFFFFu) continue;  /* a padded worklist slot */
+                row = vecs + (size_t)id * dim;
+            } else {
+                id  = 0x80000000u | (uint32_t)(c - L);
+                row = insert_list + (size_t)(c - L) * dim;
+            }
+            const float dist = vo_l2_seq(qv, row, dim);
+            /* utils.cuh:226-241: first slot holding the largest value */
+            float max_dist = -1.0f;
+            int   max_k    = 0;
+            for (int k = 0; k < L; ++k)
+                if (sd[k] > max_dist) {
+                    max_dist = sd[k];
+                    max_k    = k;
+                }
+            if (dist < max_dist) {
+                sd[max_k]  = dist;
+                sid[max_k] = id;
+            }
+        }
+        /* utils.cuh:265-283: bubble sort by distance (stable) */
+        for (int i = 0; i < L - 1; ++i)
+            for (int j = 0; j < L - i - 1; ++j)
+                if (sd[j] > sd[j + 1]) {
+                    float    td = sd[j];
+                    uint32_t ti = sid[j];
+                    sd[j]       = sd[j + 1];
+                    sid[j]      = sid[j + 1];
+                    sd[j + 1]   = td;
+                    sid[j + 1]  = ti;
+                }
+    }
+}

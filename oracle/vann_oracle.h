@@ -91,6 +91,16 @@ void vo_random_graph(int64_t n, int R, uint64_t seed, uint32_t* deg, uint32_t* a
 int64_t vo_medoid(const float* vecs, int64_t n, int dim);
 
 /* Exact kNN in FP64 (ties by id). */
+/* searchPoints2's merge (vamana/include/utils.cuh:199-285 merge_and_rerank_kernel,
+ * distances as l2_distance_sq :150-158): for each query, the L graph worklist ids
+ * then the n_il insert-list rows compete for L slots in that order.  A candidate
+ * enters when its squared distance is strictly below the largest slot value and
+ * replaces the first slot holding that value; the slots start at +inf.  The slots
+ * are then bubble-sorted by distance.  Graph candidates are reported by id, insert-
+ * list row s as 0x80000000 | s; unfilled slots as 0xFFFFFFFF with +inf. */
+void vo_merge_rerank(const float* vecs, int dim, const float* q, int64_t nq, const uint32_t* graph_ids,
+                     int L, const float* insert_list, int64_t n_il, uint32_t* out_ids, float* out_d);
+
 void vo_bruteforce_knn(const float* base, int64_t n, const float* q, int64_t nq, int dim, int k,
                        uint32_t* out_ids, double* out_d, int threads);
 

@@ -95,3 +95,49 @@ def test_insert_batch_matches_full_rebuild_shape(oracle, small):
     st, ids, d, _, _ = g.search(q, 64, 10, entry)
     truth, _ = oracle.bruteforce_knn(base, q, 10)
     assert oracle.recall_at_k(ids, truth, 10) >= 0.9
+
+
+def _merge_rerank_literal(vecs, q, graph_ids, il):
+    """merge_and_rerank_kernel (vamana/include/utils.cuh:199-285) line by line, with
+    the FP32 arithmetic of l2_distance_sq (:150-158) done exactly (integer rows)."""
+    nq, L = graph_ids.shape
+    out_i = np.full((nq, L), 0xFFFFFFFF, np.uint32)
+    out_d = np.full((nq, L), np.inf, np.float32)
+    for qi in range(nq):
+        sd = [np.inf] * L
+        si = [0xFFFFFFFF] * L
+        cands = [(int(g), vecs[g]) for g in graph_ids[qi] if g != 0xFFFFFFFF]
+        cands += [(0x80000000 | s, il[s]) for s in range(len(il))]
+        for cid, row in cands:
+            dist = float(((q[qi].astype(np.float64) - row) ** 2).sum())
+            max_d, max_k = -1.0, 0
+            for k in range(L):
+                if sd[k] > max_d:
+                    max_d, max_k = sd[k], k
+            if dist < max_d:
+                sd[max_k], si[max_k] = dist, cid
+        for i in range(L - 1):
+            for j in range(L - i - 1):
+                if sd[j] > sd[j + 1]:
+                    sd[j], sd[j + 1] = sd[j + 1], sd[j]
+                    si[j], si[j + 1] = si[j + 1], si[j]
+        out_i[qi], out_d[qi] = si, sd
+    return out_i, out_d
+
+
+def test_merge_rerank_matches_the_reference_loop(oracle):
+    """The oracle's searchPoints2 merge against a literal port of the reference's
+    loop, on small integer rows chosen to tie often (first-slot eviction matters)."""
+    rng = np.random.default_rng(12)
+    n, D, L = 300, 16, 12
+    vecs = rng.integers(0, 3, (n, D)).astype(np.float32)
+    il = rng.integers(0, 3, (40, D)).astype(np.float32)
+    q = rng.integers(0, 3, (25, D)).astype(np.float32)
+    gids = rng.integers(0, n, (25, L)).astype(np.uint32)
+    gids[:, -2:] = 0xFFFFFFFF  # padded worklist slots
+    gids[3, 1] = gids[3, 0]    # a duplicate, as the entry point gives
+    ids, d = oracle.merge_rerank(vecs, q, gids, il)
+    ri, rd = _merge_rerank_literal(vecs, q, gids, il)
+    assert np.array_equal(ids, ri)
+    assert np.array_equal(d, rd)
+    assert (ids >= oracle.STAGED).any() and (ids < oracle.STAGED).any()
