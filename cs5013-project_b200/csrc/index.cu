@@ -590,6 +590,127 @@ vann_status vann_save_graph(vann_index* h, const char* path) {
     });
 }
 
+}  // extern "C"
+
+namespace vann {
+vann_status write_bang(std::vector<unsigned char>& records, uint64_t n, uint32_t dim, uint32_t degree,
+                       uint32_t medoid, const char* out_prefix);
+}
+
+namespace {
+
+// the index's graph as the reference's records (unused slots zero)
+std::vector<unsigned char> graph_records(vann_index* h) {
+    const uint32_t        D = h->p.dim, R = h->p.degree;
+    const uint64_t        n = h->size;
+    std::vector<float>    v(n * D);
+    std::vector<uint32_t> d(n), a(n * R);
+    vann_status           s = vann_get_graph(h, v.data(), d.data(), a.data());
+    VREQUIRE(s == VANN_OK, s, g_last_error);
+    const size_t               rec = 4ull * D + 4 + 4ull * R;
+    std::vector<unsigned char> buf(rec * n);
+    for (uint64_t i = 0; i < n; ++i) {
+        unsigned char* r = buf.data() + i * rec;
+        memcpy(r, &v[i * D], 4ull * D);
+        memcpy(r + 4ull * D, &d[i], 4);
+        memset(r + 4ull * D + 4, 0, 4ull * R);
+        memcpy(r + 4ull * D + 4, &a[i * R], 4ull * d[i]);
+    }
+    return buf;
+}
+
+struct IndexFileHeader {
+    char     magic[8];
+    uint32_t version, dim, degree, consistent;
+    uint64_t size, deleted, n_free;
+    uint32_t entry, reserved;
+};
+static_assert(sizeof(IndexFileHeader) == 56, "file header layout");
+
+}  // namespace
+
+extern "C" {
+
+vann_status vann_save_graph_bang(vann_index* h, const char* out_prefix) {
+    vann_status written = VANN_OK;
+    vann_status s       = guard([&] {
+        VREQUIRE(h && out_prefix, VANN_ERR_INVALID, "null argument");
+        std::vector<unsigned char> buf = graph_records(h);
+        written = vann::write_bang(buf, h->size, h->p.dim, h->p.degree, h->entry, out_prefix);
+    });
+    return s != VANN_OK ? s : written;
+}
+
+vann_status vann_save_index(vann_index* h, const char* path) {
+    return guard([&] {
+        VREQUIRE(h && path, VANN_ERR_INVALID, "null argument");
+        const uint32_t D = h->p.dim, R = h->p.degree;
+        const uint64_t n = h->size;
+        std::vector<float>    v(n * D);
+        std::vector<uint32_t> d(n), a(n * R), tomb((n + 31) / 32);
+        vann_status           s = vann_get_graph(h, v.data(), d.data(), a.data());
+        VREQUIRE(s == VANN_OK, s, g_last_error);
+        if (n) VCHECK(cudaMemcpy(tomb.data(), h->tomb, 4 * tomb.size(), cudaMemcpyDeviceToHost));
+        for (uint64_t i = 0; i < n; ++i)  // unused slots are not part of the state
+            for (uint32_t j = d[i]; j < R; ++j) a[i * R + j] = 0;
+        IndexFileHeader hd{};
+        memcpy(hd.magic, "VANNIDX", 8);
+        hd.version    = 1;
+        hd.dim        = D;
+        hd.degree     = R;
+        hd.consistent = h->consistent ? 1u : 0u;
+        hd.size       = n;
+        hd.deleted    = h->n_deleted;
+        hd.n_free     = h->free_ids.size();
+        hd.entry      = h->entry;
+        FILE* f = fopen(path, "wb");
+        VREQUIRE(f, VANN_ERR_IO, std::string("cannot open ") + path);
+        bool ok = fwrite(&hd, sizeof(hd), 1, f) == 1;
+        ok      = ok && fwrite(v.data(), 4, v.size(), f) == v.size();
+        ok      = ok && fwrite(d.data(), 4, d.size(), f) == d.size();
+        ok      = ok && fwrite(a.data(), 4, a.size(), f) == a.size();
+        ok      = ok && fwrite(tomb.data(), 4, tomb.size(), f) == tomb.size();
+        ok      = ok && fwrite(h->free_ids.data(), 4, h->free_ids.size(), f) == h->free_ids.size();
+        ok      = fclose(f) == 0 && ok;
+        VREQUIRE(ok, VANN_ERR_IO, "short write");
+    });
+}
+
+vann_status vann_load_index(vann_index* h, const char* path) {
+    return guard([&] {
+        VREQUIRE(h && path, VANN_ERR_INVALID, "null argument");
+        FILE* f = fopen(path, "rb");
+        VREQUIRE(f, VANN_ERR_IO, std::string("cannot open ") + path);
+        IndexFileHeader hd{};
+        bool            ok = fread(&hd, sizeof(hd), 1, f) == 1;
+        if (!ok || memcmp(hd.magic, "VANNIDX", 8) != 0 || hd.version != 1) {
+            fclose(f);
+            VREQUIRE(false, VANN_ERR_IO, "not a version-1 index file");
+        }
+        if (hd.dim != h->p.dim || hd.degree != h->p.degree || hd.size > h->p.capacity ||
+            hd.n_free > hd.size || hd.deleted > hd.size) {
+            fclose(f);
+            VREQUIRE(false, VANN_ERR_INVALID, "file dim / degree / size do not fit this index");
+        }
+        const uint64_t        n = hd.size, D = hd.dim, R = hd.degree;
+        std::vector<float>    v(n * D);
+        std::vector<uint32_t> d(n), a(n * R), tomb((n + 31) / 32), fr(hd.n_free);
+        ok = fread(v.data(), 4, v.size(), f) == v.size();
+        ok = ok && fread(d.data(), 4, d.size(), f) == d.size();
+        ok = ok && fread(a.data(), 4, a.size(), f) == a.size();
+        ok = ok && fread(tomb.data(), 4, tomb.size(), f) == tomb.size();
+        ok = ok && fread(fr.data(), 4, fr.size(), f) == fr.size();
+        fclose(f);
+        VREQUIRE(ok, VANN_ERR_IO, "short read");
+        for (uint32_t x : fr) VREQUIRE(x < n, VANN_ERR_INVALID, "free id out of range");
+        vann_status s = vann_set_graph(h, v.data(), d.data(), a.data(), n, hd.entry, hd.consistent);
+        VREQUIRE(s == VANN_OK, s, g_last_error);
+        if (n) VCHECK(cudaMemcpy(h->tomb, tomb.data(), 4 * tomb.size(), cudaMemcpyHostToDevice));
+        h->n_deleted = hd.deleted;
+        h->free_ids.assign(fr.begin(), fr.end());
+    });
+}
+
 vann_status vann_build(vann_index* h, const float* d_vecs, uint64_t n, uint64_t batch, uint64_t seed,
                        uint32_t entry, void* stream) {
     return guard([&] {

@@ -35,7 +35,8 @@ EXPORTS = [
     "vann_consolidate", "vann_medoid_noalloc", "vann_server_create", "vann_server_destroy",
     "vann_server_submit_search", "vann_server_submit_insert", "vann_server_submit_delete",
     "vann_server_submit_consolidate", "vann_server_wait", "vann_server_get_stats",
-    "vann_stage_insert", "vann_search_staged", "vann_patch_graph",
+    "vann_stage_insert", "vann_search_staged", "vann_patch_graph", "vann_convert_graph_file",
+    "vann_save_graph_bang", "vann_save_index", "vann_load_index",
 ]
 
 
@@ -121,6 +122,10 @@ def lib():
             "vann_stage_insert": (C.c_int, [vp, vp, u64, vp]),
             "vann_search_staged": (C.c_int, [vp, vp, u64, C.POINTER(SearchParams), vp, vp, vp, vp]),
             "vann_patch_graph": (C.c_int, [vp, vp, vp]),
+            "vann_convert_graph_file": (C.c_int, [C.c_char_p, u64, u32, u32, u32, C.c_char_p]),
+            "vann_save_graph_bang": (C.c_int, [vp, C.c_char_p]),
+            "vann_save_index": (C.c_int, [vp, C.c_char_p]),
+            "vann_load_index": (C.c_int, [vp, C.c_char_p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -301,6 +306,17 @@ class Index:
     def consolidate(self, stream=None):
         _check(lib().vann_consolidate(self._h, _stream_ptr(stream)))
 
+    def save_graph_bang(self, prefix: str):
+        """<prefix>_disk.bin + <prefix>_disk_metadata.bin in the BANG / DiskANN layout."""
+        _check(lib().vann_save_graph_bang(self._h, prefix.encode()))
+
+    def save_index(self, path: str):
+        """Versioned full-state file: graph, tombstones, free ids, entry, consistency."""
+        _check(lib().vann_save_index(self._h, path.encode()))
+
+    def load_index(self, path: str):
+        _check(lib().vann_load_index(self._h, path.encode()))
+
     def stage_insert(self, vecs, stream=None):
         """Append rows to the insert list, outside the graph (vann_stage_insert)."""
         torch = _torch()
@@ -401,6 +417,12 @@ class Server:
         s = ServerStats()
         _check(lib().vann_server_get_stats(self._h, C.byref(s)))
         return {f: getattr(s, f) for f, _ in ServerStats._fields_}
+
+
+def convert_graph_file(in_path: str, n: int, dim: int, degree: int, medoid: int, out_prefix: str):
+    """The reference's 772-byte record file -> BANG / DiskANN disk layout, on the host
+    (what scripts/bang-preprocess.py does); no GPU needed."""
+    _check(lib().vann_convert_graph_file(in_path.encode(), n, dim, degree, medoid, out_prefix.encode()))
 
 
 def medoid_noalloc(vecs, out, stream=None):

@@ -203,6 +203,30 @@ vann_status vann_search_staged(vann_index* index, const float* d_queries, uint64
                                const vann_search_params* sp, uint32_t* d_ids, float* d_dists,
                                float* d_vecs_out, void* stream);
 
+/* On-disk interop (no counterpart call in the reference; its tooling does this in
+ * scripts/bang-preprocess.py:37-72).  BANG / DiskANN disk layout from the
+ * reference's 772-byte records: <prefix>_disk.bin holds one record per node
+ * (dim x FP32 vector, u32 degree, the degree neighbour ids sorted ascending, then
+ * the record's remaining slots unchanged); <prefix>_disk_metadata.bin holds u64
+ * medoid, u64 record bytes, u32 data type (2 = float), u32 dim, u32 degree, u32 n.
+ * Every node must have 1..degree neighbours (the script rejects others).
+ * vann_convert_graph_file converts a 772-byte record file on the host (no GPU);
+ * vann_save_graph_bang writes the index's graph (unused slots zero, as
+ * vann_save_graph writes them) with its entry point as the medoid. */
+vann_status vann_convert_graph_file(const char* in_path, uint64_t n, uint32_t dim, uint32_t degree,
+                                    uint32_t medoid, const char* out_prefix);
+vann_status vann_save_graph_bang(vann_index* index, const char* out_prefix);
+
+/* Versioned full-state file (no counterpart in the reference): the graph (any dim
+ * and degree), tombstones, ids waiting for reuse, entry point and the consistency
+ * flag, so a FreshVamana index resumes exactly.  Layout, little-endian: "VANNIDX\0",
+ * u32 version (1), u32 dim, u32 degree, u32 consistent, u64 size, u64 deleted,
+ * u64 free count, u32 entry, u32 0, then size x dim FP32 rows, size u32 degrees,
+ * size x degree u32 ids, ceil(size / 32) u32 tombstone words, free-count u32 ids.
+ * vann_load_index needs the index's dim and degree to match and capacity >= size. */
+vann_status vann_save_index(vann_index* index, const char* path);
+vann_status vann_load_index(vann_index* index, const char* path);
+
 /* The insert half of Vamana<T>::patchGraph (vamana_impl.cuh:182-265): every
  * insert-list row, in order, goes into the graph as one vann_insert batch and the
  * list is emptied.  d_ids_out (may be NULL) receives their graph ids.  Synchronises. */
