@@ -259,80 +259,114 @@ cudaError_t launch_find_vectors(const float* vecs, uint64_t n, uint32_t D, const
     return cudaGetLastError();
 }
 
-// Delete consolidation candidates (FreshDiskANN, Singh et al. 2021, Alg. 4):
-// for every live node p with a deleted out-neighbour, C = (out(p) \ D) U
-// (out(d) \ D for deleted d in out(p)), minus p, first occurrence kept, capped.
-// One warp per node; p is appended to node_list.  cand_d receives dist(p, c).
+// FreshDiskANN consolidation candidates (Algorithm 4): for each live node p with a
+// deleted out-neighbour, p's live out-neighbours in order, each deleted one
+// replaced in place by its own live out-neighbours; p itself, deleted ids and
+// repeats are skipped, and the list stops at `cap`.  One warp per node: runs of
+// live neighbours and each deleted neighbour's list go in as chunks of up to 32;
+// repeats inside a chunk fall to __match_any_sync, repeats of earlier chunks to a
+// hash set in shared memory (open addressing).  Distances are left to RobustPrune,
+// which computes them exactly.
 __global__ void consolidate_candidates_kernel(const uint32_t* deg, const uint32_t* adj, uint32_t R,
-                                              const uint32_t* tomb, uint64_t n,
-                                              uint32_t* node_list, uint32_t* n_list,
-                                              uint32_t* cand, uint32_t* cand_n, float* cand_d,
-                                              const float* vecs, uint32_t D, uint32_t cap) {
-    uint64_t p    = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
-    uint32_t lane = threadIdx.x & 31u;
-    if (p >= n) return;
-    auto dead = [&](uint32_t id) { return (tomb[id >> 5] >> (id & 31u)) & 1u; };
-    if (dead((uint32_t)p)) return;
-    uint32_t dg  = min(deg[p], R);
-    bool     any = false;
-    for (uint32_t j = lane; j < dg; j += 32) any |= dead(adj[p * R + j]) != 0;
-    if (!__any_sync(0xffffffffu, any)) return;
-    uint32_t slot = 0;
-    if (lane == 0) slot = atomicAdd(n_list, 1u);
-    slot = __shfl_sync(0xffffffffu, slot, 0);
-    if (lane == 0) node_list[slot] = (uint32_t)p;
-    uint32_t* c   = cand + (uint64_t)slot * cap;
-    uint32_t  cnt = 0;
-    // serial over out(p) in order keeps the candidate order deterministic
-    for (uint32_t j = 0; j < dg; ++j) {
-        uint32_t v = adj[p * R + j];
-        if (!dead(v)) {
-            bool dup = false;
-            for (uint32_t t = lane; t < cnt; t += 32) dup |= c[t] == v;
-            dup = __any_sync(0xffffffffu, dup);
-            if (!dup && v != (uint32_t)p && cnt < cap) {
-                if (lane == 0) c[cnt] = v;
-                ++cnt;
-            }
-            __syncwarp();
-        } else {
-            uint32_t dd = min(deg[v], R);
-            for (uint32_t k = 0; k < dd; ++k) {
-                uint32_t u = adj[(uint64_t)v * R + k];
-                if (dead(u) || u == (uint32_t)p) continue;
-                bool dup = false;
-                for (uint32_t t = lane; t < cnt; t += 32) dup |= c[t] == u;
-                dup = __any_sync(0xffffffffu, dup);
-                if (!dup && cnt < cap) {
-                    if (lane == 0) c[cnt] = u;
-                    ++cnt;
+                                              const uint32_t* tomb, uint64_t n, uint32_t* node_list,
+                                              uint32_t* n_list, uint32_t* cand, uint32_t* cand_n,
+                                              uint32_t cap, uint32_t hbits) {
+    extern __shared__ uint32_t table_all[];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t hs   = 1u << hbits;
+    uint32_t*      tab  = table_all + (threadIdx.x >> 5) * hs;
+    auto dead = [&](uint32_t id) { return (__ldg(tomb + (id >> 5)) >> (id & 31u)) & 1u; };
+    for (uint64_t p = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5); p < n;
+         p += (uint64_t)gridDim.x * (blockDim.x / 32)) {
+        if (dead((uint32_t)p)) continue;
+        const uint32_t dg = min(deg[p], R);
+        uint32_t       v  = lane < dg ? adj[p * R + lane] : kNone;
+        uint32_t       v2 = lane + 32u < dg ? adj[p * R + 32u + lane] : kNone;
+        const bool     d1 = v != kNone && dead(v), d2 = v2 != kNone && dead(v2);
+        uint32_t       dm = __ballot_sync(0xffffffffu, d1), dm2 = __ballot_sync(0xffffffffu, d2);
+        bool           any = dm != 0u || dm2 != 0u;
+        for (uint32_t j = 64; !any && j < dg; j += 32) {  // R > 64
+            const uint32_t w = j + lane < dg ? adj[p * R + j + lane] : kNone;
+            any              = __ballot_sync(0xffffffffu, w != kNone && dead(w)) != 0u;
+        }
+        if (!any) continue;
+        uint32_t slot = 0;
+        if (lane == 0) slot = atomicAdd(n_list, 1u);
+        slot = __shfl_sync(0xffffffffu, slot, 0);
+        if (lane == 0) node_list[slot] = (uint32_t)p;
+        for (uint32_t i = lane; i < hs; i += 32) tab[i] = kNone;
+        __syncwarp();
+        uint32_t* c   = cand + (uint64_t)slot * cap;
+        uint32_t  cnt = 0;
+        // one chunk: lane's id u when `valid`, appended in lane order unless seen
+        auto push = [&](uint32_t u, bool valid) {
+            const bool     ok    = valid && u != (uint32_t)p && !dead(u);
+            const uint32_t oks   = __ballot_sync(0xffffffffu, ok);
+            const uint32_t peers = __match_any_sync(0xffffffffu, ok ? u : kNone) & oks;
+            bool           fresh = false;
+            if (ok && (__ffs(peers) - 1u) == lane) {  // first lane holding u
+                uint32_t h = (u * 2654435761u) >> (32u - hbits);
+                for (uint32_t probe = 0; probe < hs; ++probe, h = (h + 1u) & (hs - 1u)) {
+                    const uint32_t old = atomicCAS(tab + h, kNone, u);
+                    if (old == kNone) {
+                        fresh = true;
+                        break;
+                    }
+                    if (old == u) break;
                 }
-                __syncwarp();
+            }
+            const uint32_t m   = __ballot_sync(0xffffffffu, fresh);
+            const uint32_t pos = cnt + __popc(m & ((1u << lane) - 1u));
+            if (fresh && pos < cap) c[pos] = u;
+            cnt = min(cap, cnt + __popc(m));
+            __syncwarp();
+        };
+        // the node's list in order, 32 entries at a time
+        for (uint32_t j0 = 0; j0 < dg && cnt < cap; j0 += 32) {
+            const uint32_t vv = j0 == 0 ? v : (j0 == 32 ? v2 : (j0 + lane < dg ? adj[p * R + j0 + lane] : kNone));
+            const bool     in = j0 + lane < dg;
+            uint32_t       deadm = j0 == 0 ? dm : (j0 == 32 ? dm2 : __ballot_sync(0xffffffffu, in && dead(vv)));
+            uint32_t       done  = 0;  // lanes of this chunk already handled
+            while (cnt < cap) {
+                const uint32_t rest = deadm & ~done;
+                const uint32_t d0   = rest ? __ffs(rest) - 1u : 32u;  // next deleted neighbour
+                const uint32_t run  = (d0 == 32u ? ~0u : ((1u << d0) - 1u)) & ~done;
+                push(vv, in && ((run >> lane) & 1u) && !((deadm >> lane) & 1u));
+                if (d0 == 32u) break;
+                done |= run | (1u << d0);
+                const uint32_t w  = __shfl_sync(0xffffffffu, vv, d0);
+                const uint32_t dw = min(deg[w], R);
+                for (uint32_t k0 = 0; k0 < dw && cnt < cap; k0 += 32) {
+                    const bool kin = k0 + lane < dw;
+                    push(kin ? adj[(uint64_t)w * R + k0 + lane] : kNone, kin);
+                }
             }
         }
+        if (lane == 0) cand_n[slot] = cnt;
+        __syncwarp();
     }
-    // distances to p
-    for (uint32_t t = 0; t < cnt; ++t) {
-        const float* a = vecs + (uint64_t)p * D;
-        const float* b = vecs + (uint64_t)c[t] * D;
-        float        s = 0.f;
-        for (uint32_t d = lane; d < D; d += 32) {
-            float x = a[d] - b[d];
-            s       = fmaf(x, x, s);
-        }
-        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) cand_d[(uint64_t)slot * cap + t] = s;
-    }
-    if (lane == 0) cand_n[slot] = cnt;
 }
 cudaError_t launch_consolidate_candidates(const uint32_t* deg, const uint32_t* adj, uint32_t R,
                                           const uint32_t* tomb, uint64_t n, uint32_t* node_list,
-                                          uint32_t* n_list, uint32_t* cand, uint32_t* cand_n,
-                                          float* cand_d, const float* vecs, uint32_t D,
-                                          uint32_t cap, cudaStream_t st) {
+                                          uint32_t* n_list, uint32_t* cand, uint32_t* cand_n, uint32_t cap,
+                                          int num_sms, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
-    consolidate_candidates_kernel<<<(unsigned)((n + 3) / 4), 128, 0, st>>>(
-        deg, adj, R, tomb, n, node_list, n_list, cand, cand_n, cand_d, vecs, D, cap);
+    uint32_t hbits = 5;
+    while ((1u << hbits) < 2u * cap) ++hbits;  // load factor <= 1/2
+    const int    warps = 4;
+    const size_t smem  = sizeof(uint32_t) * warps * (1u << hbits);
+    cudaError_t  e = cudaFuncSetAttribute(consolidate_candidates_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e          = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, consolidate_candidates_kernel, warps * 32, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    uint64_t grid = (uint64_t)per_sm * num_sms;
+    const uint64_t need = (n + warps - 1) / warps;
+    if (grid > need) grid = need;
+    consolidate_candidates_kernel<<<(unsigned)grid, warps * 32, smem, st>>>(deg, adj, R, tomb, n, node_list,
+                                                                            n_list, cand, cand_n, cap, hbits);
     return cudaGetLastError();
 }
 

@@ -140,7 +140,7 @@ struct vann_index {
     }
 
     DevBuf vis_ids, vis_d, vis_n, nodes, runs, ovf, stage, s2_ids, s2_d, e_keys, e_vals, e_keys2, e_vals2, counts, offsets, cub_tmp,
-        medoid_ws, gather, cand, cand_n, cand_d, list_n, out_tmp;
+        medoid_ws, gather, cand, cand_n, list_n, out_tmp;
 
     void alloc(void** ptr, size_t bytes) {
         VCHECK(cudaMalloc(ptr, bytes));
@@ -157,7 +157,7 @@ struct vann_index {
         cudaFree(counters);
         cudaFree(status);
         for (DevBuf* b : {&vis_ids, &vis_d, &vis_n, &nodes, &runs, &ovf, &stage, &s2_ids, &s2_d, &e_keys, &e_vals, &e_keys2, &e_vals2,
-                          &counts, &offsets, &cub_tmp, &medoid_ws, &gather, &cand, &cand_n, &cand_d,
+                          &counts, &offsets, &cub_tmp, &medoid_ws, &gather, &cand, &cand_n,
                           &list_n, &out_tmp})
             b->release();
     }
@@ -1051,13 +1051,12 @@ vann_status vann_consolidate(vann_index* h, void* stream) {
         h->nodes.ensure(sizeof(uint32_t) * h->size);
         h->list_n.ensure(sizeof(uint32_t) * 4);
         h->cand.ensure(sizeof(uint32_t) * h->size * cap);
-        h->cand_d.ensure(sizeof(float) * h->size * cap);
         h->cand_n.ensure(sizeof(uint32_t) * h->size);
         VCHECK(cudaMemsetAsync(h->list_n.p, 0, sizeof(uint32_t), st));
         VCHECK(vann::launch_consolidate_candidates(h->deg, h->adj, R, h->tomb, h->size,
                                                    h->nodes.as<uint32_t>(), h->list_n.as<uint32_t>(),
-                                                   h->cand.as<uint32_t>(), h->cand_n.as<uint32_t>(),
-                                                   h->cand_d.as<float>(), h->vecs, h->p.dim, cap, st));
+                                                   h->cand.as<uint32_t>(), h->cand_n.as<uint32_t>(), cap,
+                                                   h->num_sms, st));
         uint32_t nlist = 0;
         VCHECK(cudaMemcpyAsync(&nlist, h->list_n.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         VCHECK(cudaStreamSynchronize(st));
@@ -1073,7 +1072,7 @@ vann_status vann_consolidate(vann_index* h, void* stream) {
         pa.node_ids = h->nodes.as<uint32_t>();
         pa.n_nodes = nlist;
         pa.a_ids = h->cand.as<uint32_t>();
-        pa.a_d = h->cand_d.as<float>();
+        pa.a_d = nullptr;  // computed by the prune
         pa.a_n = h->cand_n.as<uint32_t>();
         pa.a_stride = cap;
         pa.use_b = 0;

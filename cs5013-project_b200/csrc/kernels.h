@@ -60,7 +60,8 @@ struct PruneArgs {
     // nodes to prune: node_ids[i] for i < n_nodes, or all ids < n_nodes when null
     const uint32_t* node_ids;
     uint64_t        n_nodes;
-    // A as per-node lists (out-prune): a_ids/a_d [n_nodes x a_stride], a_n
+    // A as per-node lists (out-prune): a_ids/a_d [n_nodes x a_stride], a_n;
+    // a_d null: the distances to the node are computed here
     const uint32_t* a_ids;
     const float*    a_d;
     const uint32_t* a_n;
@@ -129,8 +130,7 @@ cudaError_t launch_find_vectors(const float* vecs, uint64_t n, uint32_t D, const
                                 uint64_t nq, const uint32_t* tomb, int32_t* out, cudaStream_t st);
 cudaError_t launch_consolidate_candidates(const uint32_t* deg, const uint32_t* adj, uint32_t R,
                                           const uint32_t* tomb, uint64_t n, uint32_t* node_list,
-                                          uint32_t* n_list, uint32_t* cand, uint32_t* cand_n,
-                                          float* cand_d, const float* vecs, uint32_t D,
-                                          uint32_t cap, cudaStream_t st);
+                                          uint32_t* n_list, uint32_t* cand, uint32_t* cand_n, uint32_t cap,
+                                          int num_sms, cudaStream_t st);
 
 }  // namespace vann

@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
                         id = __ldg(a.csr_src + aoff + i);
                     } else {
                         id = __ldg(a.a_ids + (uint64_t)w * a.a_stride + i);
-                        d  = __ldg(a.a_d + (uint64_t)w * a.a_stride + i);
+                        if (a.a_d) d = __ldg(a.a_d + (uint64_t)w * a.a_stride + i);
                     }
                 } else {
                     id = __ldg(a.adj + (uint64_t)node * R + (i - nA));
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
             }
             __syncwarp();
             // distances to the node for the reverse sources and B
-            const uint32_t dstart = rev ? 0u : nA;
+            const uint32_t dstart = (rev || a.a_d == nullptr) ? 0u : nA;
             constexpr int  G      = Layout<StoreF32, DC>::kG;
             for (uint32_t g0 = dstart; g0 < nc; g0 += G) {
                 int      gc = (int)min((uint32_t)G, nc - g0);

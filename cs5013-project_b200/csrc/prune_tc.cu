@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(kThreads) prune_tc_kernel(PruneArgs a, uint32_
             if (tid == 0) out_list[atomicAdd(out_count, 1u)] = w;
             continue;
         }
-        const bool computed = rev || nB > 0;  // some distance to the node is not given
+        const bool computed = rev || nB > 0 || a.a_d == nullptr;  // some distance is not given
 
         // --- 1. candidate ids (A then B) and given distances; the node's row
         for (uint32_t i = tid; i < nc; i += kThreads) {
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(kThreads) prune_tc_kernel(PruneArgs a, uint32_
                     id = __ldg(a.csr_src + aoff + i);
                 } else {
                     id = __ldg(a.a_ids + (uint64_t)w * a.a_stride + i);
-                    d  = __ldg(a.a_d + (uint64_t)w * a.a_stride + i);
+                    if (a.a_d) d = __ldg(a.a_d + (uint64_t)w * a.a_stride + i);
                 }
             } else {
                 id = __ldg(a.adj + (uint64_t)node * R + (i - nA));

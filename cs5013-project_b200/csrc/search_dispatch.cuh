@@ -9,7 +9,7 @@ namespace vann {
 
 // Launch-bound variants (minimum resident blocks per SM, i.e. a register cap)
 // exist for the common shape (D <= 128, R <= 64); the autotuner picks one.
-constexpr int kSearchVariants = 5;
+constexpr int kSearchVariants = 7;
 
 template <typename S, int DC, int SPL>
 static cudaError_t launch_v(const SearchArgs& a, int variant, int sms, cudaStream_t st) {
@@ -21,6 +21,8 @@ static cudaError_t launch_v(const SearchArgs& a, int variant, int sms, cudaStrea
                 case 2: return launch_rw<S, DC, SPL, 1, 5>(a, sms, st);
                 case 3: return launch_rw<S, DC, SPL, 1, 7>(a, sms, st);
                 case 4: return launch_rw<S, DC, SPL, 1, 8>(a, sms, st);
+                case 5: return launch_rw<S, DC, SPL, 1, 9>(a, sms, st);
+                case 6: return launch_rw<S, DC, SPL, 1, 10>(a, sms, st);
                 default: return launch_rw<S, DC, SPL, 1, 6>(a, sms, st);
             }
         }
@@ -30,6 +32,8 @@ static cudaError_t launch_v(const SearchArgs& a, int variant, int sms, cudaStrea
                 case 2: return launch_rw<S, DC, SPL, 2, 5>(a, sms, st);
                 case 3: return launch_rw<S, DC, SPL, 2, 7>(a, sms, st);
                 case 4: return launch_rw<S, DC, SPL, 2, 8>(a, sms, st);
+                case 5: return launch_rw<S, DC, SPL, 2, 9>(a, sms, st);
+                case 6: return launch_rw<S, DC, SPL, 2, 10>(a, sms, st);
                 default: return launch_rw<S, DC, SPL, 2, 6>(a, sms, st);
             }
         }
@@ -38,6 +42,8 @@ static cudaError_t launch_v(const SearchArgs& a, int variant, int sms, cudaStrea
             case 2: return launch_t<S, DC, SPL, 5>(a, sms, st);
             case 3: return launch_t<S, DC, SPL, 7>(a, sms, st);
             case 4: return launch_t<S, DC, SPL, 8>(a, sms, st);
+            case 5: return launch_t<S, DC, SPL, 9>(a, sms, st);
+            case 6: return launch_t<S, DC, SPL, 10>(a, sms, st);
             default: break;
         }
     }
