@@ -187,20 +187,46 @@ struct vann_index {
 
     // RobustPrune launch: the tensor-core pass when an exact uint8 copy exists
     // (decided on the device by the exactness flag), prune_kernel for the rest
+    // RobustPrune launch.  Consistent reverse re-prunes go first to the warp-per-node
+    // kernel; the tensor-core passes take what it hands on (or every node) when an
+    // exact uint8 copy may exist (decided on the device by the exactness flag);
+    // prune_kernel finishes whatever is left.
     void run_prune(vann::PruneArgs pa, cudaStream_t st) {
         if (pa.n_nodes == 0) return;
         pa.pruned = reinterpret_cast<unsigned long long*>(status + vann::kWordPruned);
-        if (store[3] && vann::prune_tc_supported(p.dim, p.degree)) {
-            ovf.ensure(sizeof(uint32_t) * (3 * pa.n_nodes + 4));
-            pa.vecs_u8  = static_cast<const uint8_t*>(store[3]);
-            pa.gate     = u8_inexact();
-            pa.in_list  = ovf.as<uint32_t>();
-            pa.in_count = status + vann::kWordOverflow;
+        const uint64_t n   = pa.n_nodes;
+        const bool     tc  = store[3] && vann::prune_tc_supported(p.dim, p.degree);
+        const bool     rev = pa.consistent && pa.csr_off && pa.node_ids && p.dim <= 256;
+        if (store[3]) {
+            pa.vecs_u8 = static_cast<const uint8_t*>(store[3]);
+            pa.gate    = u8_inexact();
+        }
+        // lists: [0, n] rev hand-off + count, [n+1, 2n+2) final hand-off + count, then tc scratch
+        ovf.ensure(sizeof(uint32_t) * (4 * n + 8));
+        uint32_t*       rev_list   = ovf.as<uint32_t>();
+        uint32_t*       rev_count  = rev_list + n;
+        uint32_t*       last_list  = rev_list + n + 1;
+        uint32_t*       last_count = last_list + n;
+        uint32_t*       ws         = last_count + 1;
+        const uint32_t* in_list    = nullptr;  // every node
+        const uint32_t* in_count   = nullptr;
+        if (rev) {
+            VCHECK(cudaMemsetAsync(rev_count, 0, sizeof(uint32_t), st));
+            VCHECK(vann::launch_prune_rev(pa, rev_list, rev_count, num_sms, st));
+            pa.counter = next_counter(st);
+            in_list    = rev_list;
+            in_count   = rev_count;
+        }
+        if (tc) {
             uint32_t* tc_counters = next_counter(st);  // one per pass
             VCHECK(cudaMemsetAsync(tc_counters + 1, 0, 2 * sizeof(uint32_t), st));
-            VCHECK(vann::launch_prune_tc(pa, ovf.as<uint32_t>() + pa.n_nodes, tc_counters, num_sms, st));
-            pa.counter = next_counter(st);
+            VCHECK(vann::launch_prune_tc(pa, in_list, in_count, last_list, last_count, ws, tc_counters, num_sms,
+                                         st));
+            in_list  = last_list;
+            in_count = last_count;
         }
+        pa.in_list  = in_list;
+        pa.in_count = in_count;
         VCHECK(vann::launch_prune(pa, num_sms, st));
     }
 

@@ -77,20 +77,26 @@ struct PruneArgs {
     int             consistent;  // B lists are alpha-consistent: skip B-B checks
     uint32_t*       counter;     // work counter, zeroed before launch
     uint32_t*       status;
-    // tensor-core passes (prune_tc.cu) and their hand-off to prune_kernel
-    const uint8_t*  vecs_u8;     // exact uint8 rows
+    // tensor-core passes (prune_tc.cu) and the hand-off between kernels
+    const uint8_t*  vecs_u8;     // exact uint8 rows (or null)
     const uint32_t* gate;        // non-zero: the uint8 rows are not exact
-    uint32_t*       in_list;     // slots (positions in node_ids) left to prune_kernel
-    uint32_t*       in_count;
+    const uint32_t* in_list;     // prune_kernel: only the slots in_list[0 .. *in_count) (when set)
+    const uint32_t* in_count;
     unsigned long long* pruned;  // [0] tensor-core, [1] CUDA-core node counts (or null)
 };
 
-// prune_kernel: with gate == null every node; otherwise every node when *gate
-// is set, else only the in_list slots the tensor-core passes handed over.
+// prune_kernel: every node, or the listed slots when a.in_count is set.
 cudaError_t launch_prune(const PruneArgs& a, int num_sms, cudaStream_t st);
 bool        prune_tc_supported(uint32_t D, uint32_t R);
-// ws: 2 * n_nodes + 4 words of scratch; counters: three zeroed work counters
-cudaError_t launch_prune_tc(const PruneArgs& a, uint32_t* ws, uint32_t* counters, int num_sms, cudaStream_t st);
+// Tensor-core passes over in_list (every node when null); leftovers to out_list.
+// ws: 2 * n_nodes + 4 words of scratch; counters: three zeroed work counters.
+cudaError_t launch_prune_tc(const PruneArgs& a, const uint32_t* in_list, const uint32_t* in_count,
+                            uint32_t* out_list, uint32_t* out_count, uint32_t* ws, uint32_t* counters, int num_sms,
+                            cudaStream_t st);
+// Reverse re-prune of consistent lists, one warp per node (prune_rev.cu): nodes
+// with more than 128 candidates or 8 reverse sources are handed on in out_list.
+cudaError_t launch_prune_rev(const PruneArgs& a, uint32_t* out_list, uint32_t* out_count, int num_sms,
+                             cudaStream_t st);
 
 // searchPoints2's merge of graph results with the insert list (staged.cu)
 struct StagedArgs {

@@ -56,9 +56,8 @@ __global__ void __launch_bounds__(128) prune_kernel(PruneArgs a, uint32_t p2, ui
     const uint32_t R    = a.R;
     uint32_t*      plist  = chosen + R;  // positions of one round's candidates
     const bool     rev  = a.csr_off != nullptr;
-    // paired with the tensor-core passes: all nodes if they stood down, else the
-    // large nodes they handed over, one per warp
-    const bool     all   = a.gate == nullptr || *reinterpret_cast<volatile const uint32_t*>(a.gate) != 0u;
+    // every node, or the nodes other kernels handed over (large ones: one per warp)
+    const bool     all   = a.in_count == nullptr;
     const uint64_t nwork = all ? a.n_nodes : (uint64_t)*reinterpret_cast<volatile const uint32_t*>(a.in_count);
     if (!all) chunk = 1u;
 

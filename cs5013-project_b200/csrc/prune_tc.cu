@@ -146,9 +146,13 @@ __global__ void __launch_bounds__(kThreads) prune_tc_kernel(PruneArgs a, uint32_
     constexpr uint32_t KPT = MAXC / kThreads;  // sort keys per thread
     extern __shared__ __align__(1024) unsigned char smem[];
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    if (*reinterpret_cast<volatile const uint32_t*>(a.gate) != 0u) return;  // uniform: rows not exact
     const uint64_t nwork = in_list ? (uint64_t)*reinterpret_cast<volatile const uint32_t*>(in_count) : a.n_nodes;
     if (nwork == 0) return;
+    if (*reinterpret_cast<volatile const uint32_t*>(a.gate) != 0u) {  // rows not exact: hand every node on
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + tid; i < nwork; i += (uint64_t)gridDim.x * blockDim.x)
+            out_list[atomicAdd(out_count, 1u)] = in_list ? __ldg(in_list + i) : (uint32_t)i;
+        return;
+    }
 
     const uint32_t D = a.D, R = a.R;
     const TcLayout lay = TcLayout::make(D, MAXC);
@@ -552,12 +556,15 @@ cudaError_t launch_tc(const PruneArgs& a, uint32_t* counter, const uint32_t* in_
 }  // namespace
 
 // Passes of 256 candidates (4 CTAs per SM), then 512 (2 per SM), then 768 (one per
-// SM, when its shared memory fits: D <= 128) for the nodes each pass handed over;
-// larger ones are left in a.in_list for prune_kernel.
+// SM, when its shared memory fits: D <= 160), each over the nodes the previous one
+// handed on.  The first pass takes in_list[0 .. *in_count) (every node when null);
+// what the last cannot take goes to out_list for prune_kernel.
 // ws: 2 * n_nodes + 4 words of device scratch; counters: three zeroed work counters.
-cudaError_t launch_prune_tc(const PruneArgs& a, uint32_t* ws, uint32_t* counters, int num_sms, cudaStream_t st) {
+cudaError_t launch_prune_tc(const PruneArgs& a, const uint32_t* in_list, const uint32_t* in_count,
+                            uint32_t* out_list, uint32_t* out_count, uint32_t* ws, uint32_t* counters, int num_sms,
+                            cudaStream_t st) {
     if (a.n_nodes == 0) return cudaSuccess;
-    if (!prune_tc_supported(a.D, a.R) || !a.vecs_u8 || !a.gate || !a.in_list || !a.in_count)
+    if (!prune_tc_supported(a.D, a.R) || !a.vecs_u8 || !a.gate || !out_list || !out_count)
         return cudaErrorInvalidValue;
     int dev = 0, max_optin = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -567,17 +574,17 @@ cudaError_t launch_prune_tc(const PruneArgs& a, uint32_t* ws, uint32_t* counters
     const bool third  = TcLayout::make(a.D, 768).bytes <= (uint32_t)max_optin;
     uint32_t*  list1  = ws;
     uint32_t*  count1 = ws + a.n_nodes;
-    uint32_t*  list2  = third ? ws + a.n_nodes + 1 : a.in_list;
-    uint32_t*  count2 = third ? ws + 2 * a.n_nodes + 1 : a.in_count;
-    for (uint32_t* c : {count1, count2, a.in_count}) {
+    uint32_t*  list2  = third ? ws + a.n_nodes + 1 : out_list;
+    uint32_t*  count2 = third ? ws + 2 * a.n_nodes + 1 : out_count;
+    for (uint32_t* c : {count1, count2, out_count}) {
         e = cudaMemsetAsync(c, 0, sizeof(uint32_t), st);
         if (e != cudaSuccess) return e;
     }
-    e = launch_tc<256>(a, counters, nullptr, nullptr, list1, count1, a.n_nodes, num_sms, st);
+    e = launch_tc<256>(a, counters, in_list, in_count, list1, count1, a.n_nodes, num_sms, st);
     if (e != cudaSuccess) return e;
     e = launch_tc<512>(a, counters + 1, list1, count1, list2, count2, a.n_nodes, num_sms, st);
     if (e != cudaSuccess || !third) return e;
-    return launch_tc<768>(a, counters + 2, list2, count2, a.in_list, a.in_count, a.n_nodes, num_sms, st);
+    return launch_tc<768>(a, counters + 2, list2, count2, out_list, out_count, a.n_nodes, num_sms, st);
 }
 
 }  // namespace vann
