@@ -171,10 +171,25 @@ struct vann_index {
     uint64_t tomb_words() const { return (p.capacity + 31) / 32; }
 
     uint32_t* u8_inexact() const { return status + vann::kWordU8Inexact; }
+    int       u8_state = -1;  // exactness of the uint8 copy seen by the host: -1 unknown, 0 no, 1 yes
+
+    // whether every row is exact in the uint8 copy (read from the device once after
+    // the rows change)
+    bool u8_exact(cudaStream_t st) {
+        if (!store[3]) return false;
+        if (u8_state < 0) {
+            uint32_t f = 0;
+            VCHECK(cudaMemcpyAsync(&f, u8_inexact(), sizeof(f), cudaMemcpyDeviceToHost, st));
+            VCHECK(cudaStreamSynchronize(st));
+            u8_state = f == 0u ? 1 : 0;
+        }
+        return u8_state == 1;
+    }
 
     // rows [first, first + rows) -> traversal copies; rows from 0 replace every
     // row, so the uint8 exactness flag starts over
     void convert_rows(uint64_t first, uint64_t rows, cudaStream_t st) {
+        u8_state = -1;
         if (first == 0) VCHECK(cudaMemsetAsync(u8_inexact(), 0, sizeof(uint32_t), st));
         for (int s = 1; s < 4; ++s) {
             if (!store[s]) continue;
@@ -287,7 +302,13 @@ struct vann_index {
         a.max_visited = MV;
         a.counter = next_counter(st);
         a.status = status;
-        VCHECK(vann::launch_search(a, 0, num_sms, st));
+        // exact uint8 rows give the FP32 distances bit for bit from a quarter of the bytes
+        int sstore = VANN_STORE_F32;
+        if (u8_exact(st)) {
+            a.store = store[3];
+            sstore  = VANN_STORE_U8;
+        }
+        VCHECK(vann::launch_search(a, sstore, num_sms, st));
 
         vann::PruneArgs pa{};
         pa.vecs = vecs;
@@ -1004,6 +1025,7 @@ vann_status vann_insert(vann_index* h, const float* d_vecs, uint64_t n, uint32_t
         if (reuse == 0) {
             h->convert_rows(h->size, n, st);
         } else {
+            h->u8_state = -1;
             for (int s = 1; s < 4; ++s)  // reused ids are scattered: convert by id list
                 if (h->store[s])
                     VCHECK(vann::launch_convert_ids(h->vecs, h->nodes.as<uint32_t>(), n, h->store[s],
