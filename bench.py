@@ -148,10 +148,33 @@ def build_index(torch, vann, base_d, dev):
     return idx, time.time() - t0
 
 
-def time_steps(torch, fn, steps, warmup, flush):
+def max_over_ranks(torch, dist, values, device):
+    """Each value's maximum over the ranks (one all_reduce); as given without ranks."""
+    if dist is None:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def replica_throughput(world, units_per_rank, max_seconds):
+    """Whole-job rate of `world` replicas that each did units_per_rank, timed as the
+    slowest rank."""
+    return world * units_per_rank / max_seconds
+
+
+def ranks_aligned(torch, dist):
+    """Device idle and every rank at the same point (the bracket of a timed region)."""
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def time_steps(torch, fn, steps, warmup, flush, dist=None):
     for _ in range(warmup):
         fn()
-    torch.cuda.synchronize()
+    ranks_aligned(torch, dist)
     st = torch.cuda.current_stream()
     times = []
     for _ in range(steps):
@@ -163,6 +186,7 @@ def time_steps(torch, fn, steps, warmup, flush):
         e1.record(st)
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
+    ranks_aligned(torch, dist)
     return times
 
 
@@ -234,7 +258,7 @@ def main():
             name = store + ("+rerank" if rr else "")
             L, r = op_point(name)
             fn = lambda s=store, rr=rr, L=L: idx.search(q_d, k=K, L=L, store=s, rerank=rr, out=out)
-            t = time_steps(torch, fn, steps, warm, flush)
+            t = time_steps(torch, fn, steps, warm, flush, dist)
             results[name] = {"L": L, "recall": r, "ms": t}
     clocks = clk.summary()
 
@@ -323,12 +347,13 @@ def main():
                 ev_out[bsel].record(s_out)
 
     e2e_run(warm)
-    torch.cuda.synchronize()
+    ranks_aligned(torch, dist)
     e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e_start.record(s_in)
     e2e_run(steps)
     e_end.record(s_out)  # after the last download
     e_end.synchronize()
+    ranks_aligned(torch, dist)
     e2e_total_ms = e_start.elapsed_time(e_end)
     e2e_ms = [e2e_total_ms / steps] * steps
     e2e_qps = nq * steps / (e2e_total_ms / 1e3)
@@ -337,14 +362,9 @@ def main():
     assert torch.equal(got, obuf[(steps - 1) % 2][0].cpu().to(torch.int64))
 
     # ---- max over ranks
-    total_s = sum(hr["ms"]) / 1e3
-    if dist is not None:
-        t = torch.tensor([total_s, sum(e2e_ms) / 1e3], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_s, e2e_total = t.tolist()
-        e2e_qps = world * nq * steps / e2e_total
-        dist.barrier()
-    value = world * nq * steps / total_s
+    total_s, e2e_total = max_over_ranks(torch, dist, [sum(hr["ms"]) / 1e3, sum(e2e_ms) / 1e3], dev)
+    value   = replica_throughput(world, nq * steps, total_s)
+    e2e_qps = replica_throughput(world, nq * steps, e2e_total)
 
     # ---- CPU baseline: the oracle's search (same semantics as the FP32 form)
     cpu = None
