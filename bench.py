@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile", action="store_true", help="short run for a profiler capture")
+    ap.add_argument("--only", default=None,
+                    help="FORM@L (e.g. u8@32): sweep and time that one form at that L only, no autotune "
+                         "(a profiler capture of exactly one kernel instantiation)")
     ap.add_argument("--config", default="search", choices=["search", "churn", "precision", "serve", "build"],
                     help="search: the headline line; churn / precision / serve: configurations 3-5; "
                          "build: index build and insert throughput (their own JSON lines)")
@@ -223,9 +226,14 @@ def main():
     # ---- sweep
     sweep = {}
     forms = [("f32", False), ("bf16", False), ("u8", False), ("fp8", True)]
+    sweep_L = L_SWEEP
+    if args.only:
+        oname, oL = args.only.split("@")
+        forms = [f for f in forms if f[0] + ("+rerank" if f[1] else "") == oname]
+        sweep_L = [int(oL)]
     for store, rr in forms:
         name = store + ("+rerank" if rr else "")
-        for L in L_SWEEP:
+        for L in sweep_L:
             ids, _ = idx.search(q_d, k=K, L=L, store=store, rerank=rr)
             torch.cuda.synchronize()
             sweep.setdefault(name, []).append((L, recall(torch, ids, gt)))
@@ -288,7 +296,7 @@ def main():
         return float(per_q.sum()), float(hops.mean()), float(evals.mean())
 
     bytes_head, hops_head, evals_head = counted_bytes(head)
-    bytes_f32, hops_f32, evals_f32 = counted_bytes("f32")
+    hops_f32 = counted_bytes("f32")[1] if "f32" in results else None
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -368,7 +376,7 @@ def main():
 
     # ---- CPU baseline: the oracle's search (same semantics as the FP32 form)
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and "f32" in results:
         cpu = cpu_baseline(idx, q, results["f32"]["L"], args.cpu_sample, hops_f32, args.cpu_seconds)
 
     if rank == 0:
@@ -386,7 +394,7 @@ def main():
             "p50_ms": round(p50, 4), "p99_ms": round(p99, 4),
             "forms": {nm: {"L": v["L"], "recall@10": round(v["recall"], 4), "qps": round(qps(nm), 1),
                            "p99_ms": round(float(np.percentile(v["ms"], 99)), 4)} for nm, v in results.items()},
-            "speedup_vs_fp32_plain": round(qps(head) / qps("f32"), 3),
+            "speedup_vs_fp32_plain": round(qps(head) / qps("f32"), 3) if "f32" in results else None,
             "autotune_ms_per_variant": tune_ms,
             "sweep": {nm: [[L, round(r, 4)] for L, r in v] for nm, v in sweep.items()},
             "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": nq * DIM * 4,
