@@ -118,3 +118,35 @@ def test_consolidate_equals_cuda_core_path(vann_mod):
     _, da, aa = tc.get_graph()
     _, db, ab = cc.get_graph()
     assert _rows_equal(da, aa, db, ab) == []
+
+
+@pytest.mark.parametrize("D", [64, 256])
+def test_other_dims_match_oracle(oracle, vann_mod, D):
+    """D=64 (two K steps per Gram tile) and D=256 (eight K steps, 256-byte rows, the
+    wide warp layouts): batched build and insert, every prune path, against the oracle."""
+    import torch
+
+    n, B, R, L = 3000, 1000, 32, 64
+    base = workload.mixture(n + 300, D, 30, seed=49)
+    deg0, adj0 = oracle.random_graph(B, R, 13)
+    deg = np.zeros(n + 300, np.uint32)
+    adj = np.zeros((n + 300, R), np.uint32)
+    deg[:B], adj[:B] = deg0, adj0
+    og = oracle.Graph(base, deg, adj)
+    entry = oracle.medoid(base[:B])
+    assert og.vamana_batch(0, B, L, 1.2, entry, skip_mode=2) == 0
+    for s in range(B, n, B):
+        assert og.vamana_batch(s, B, L, 1.2, entry, skip_mode=0) == 0
+    assert og.vamana_batch(n, 300, L, 1.2, entry, skip_mode=0) == 0
+    idx = vann_mod.Index(D, R, L, 1.2, capacity=n + 300, stores=("f32", "u8"))
+    idx.build(torch.from_numpy(base[:n]).cuda(), batch=B, seed=13)
+    idx.insert(torch.from_numpy(base[n:]).cuda())
+    info = idx.info()
+    assert info["pruned_tc"] > 0 and info["pruned_cuda"] > 0
+    _, gdeg, gadj = idx.get_graph()
+    assert _rows_equal(gdeg, gadj, og.deg, og.adj) == []
+    q = workload.mixture(100, D, 30, seed=50)
+    ids, d = idx.search(torch.from_numpy(q).cuda(), k=10, L=48, store="u8")
+    st, oids, od, _, _ = og.search(q, 48, 10, entry, bloom_mode=oracle.BLOOM_SNAPSHOT)
+    assert np.array_equal(ids.cpu().numpy().view(np.uint32), oids)
+    assert np.array_equal(d.cpu().numpy(), od)
