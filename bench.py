@@ -2,18 +2,19 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload (configuration 2 of the reference benchmark plan): 1,000,000 base
+Workload: 1,000,000 base
 vectors x 128 dims, integer-valued FP32 from a clipped 1,000-cluster Gaussian
 mixture (seeded, synthetic: no dataset is read), 10,000 queries; the index is
 built on the GPU with R=64, L=100, alpha=1.2 in batched inserts of 10,000.
 Ground truth is FP64 brute force.  Search L is swept; each form's operating
 point is the smallest L whose recall@10 >= 0.95.
 
-A step is one batched search of the 10,000 queries.  `value` is the headline
-form's (reduced-precision traversal + exact FP32 rerank) queries/s, device time
-with CUDA events on the launching stream, L2 flushed before every step.
-`e2e` repeats it through the public C ABI with pinned host buffers: each step
-copies the queries in and the ids/distances out inside the timed region.
+A step is one batched search of the 10,000 queries.  `value` is the queries/s of
+the fastest reduced-precision form at recall@10 >= 0.95 (uint8 or BF16 traversal
+copies, or FP8 traversal with an exact FP32 rerank), device time with CUDA events
+on the launching stream, L2 flushed before every step.  `e2e` repeats it through
+the public C ABI with pinned host buffers: each step copies the queries in and the
+ids/distances out inside the timed region, the L2 flushed before every search.
 
 Multi-GPU: replicas only -- every rank builds the same index and searches its
 own full query batch; value = all ranks' queries / max-over-ranks time.
@@ -60,8 +61,9 @@ def parse():
                     help="FORM@L (e.g. u8@32): sweep and time that one form at that L only, no autotune "
                          "(a profiler capture of exactly one kernel instantiation)")
     ap.add_argument("--config", default="search", choices=["search", "churn", "precision", "serve", "build"],
-                    help="search: the headline line; churn / precision / serve: configurations 3-5; "
-                         "build: index build and insert throughput (their own JSON lines)")
+                    help="search: the headline line; churn / precision / serve: FreshVamana churn on 1M, "
+                         "reduced precision on 5M x 96, serving on 10M; build: index build and insert "
+                         "throughput (each its own JSON line)")
     ap.add_argument("--rounds", type=int, default=20)
     ap.add_argument("--rate", type=float, default=50_000.0, help="serve: offered requests/s")
     ap.add_argument("--duration", type=float, default=5.0, help="serve: seconds of arrivals")
@@ -597,7 +599,7 @@ def main_precision():
     from vann import workload
 
     dev = torch.device("cuda", 0)
-    n = args.n if "--n" in sys.argv else 5_000_000  # configuration 4 is 5M rows
+    n = args.n if "--n" in sys.argv else 5_000_000  # the 5M x 96 float workload
     nq, D = args.nq, 96
     base = workload.mixture(n, D, 2000, seed=11, sigma=0.05, integer=False, unit_norm=True)
     q = workload.mixture(nq, D, 2000, seed=12, sigma=0.05, integer=False, unit_norm=True)
@@ -648,7 +650,7 @@ def main_precision():
 
 
 def main_serve():
-    """Serving: a uint8 index (configuration 5: 10M x 128, 4,000 clusters, R=64) behind the
+    """Serving: a uint8 index (10M x 128, 4,000 clusters, R=64) behind the
     continuous-batching server; a Poisson stream of requests at --rate: searches of one
     query with k in {1, 10, 100} and L uniform in 16..512, and write requests (insert or
     delete batches, size log-uniform in 1..max-write).  Reports achieved throughput,
@@ -662,7 +664,7 @@ def main_serve():
     from vann import workload
 
     dev = torch.device("cuda", 0)
-    n = args.n if "--n" in sys.argv else 10_000_000  # configuration 5 is 10M rows
+    n = args.n if "--n" in sys.argv else 10_000_000  # the 10M x 128 serving workload
     clusters = 4000 if n >= 1_000_000 else max(10, n // 2500)
     base = workload.mixture(n, DIM, clusters, seed=1)
     qpool = workload.mixture(20_000, DIM, clusters, seed=2)
