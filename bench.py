@@ -304,7 +304,10 @@ def main():
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except OSError:
         pass
+    # the measured copy bandwidth of this pool's B200s; else the earlier measurement
     peak = peaks.get("hbm_gbs", 6650.0)
+    peak_source = ("MEASURED_PEAKS.json hbm_gbs (burst), of measured" if "hbm_gbs" in peaks
+                   else "fallback 6650 GB/s (no MEASURED_PEAKS.json), of fallback")
     achieved = bytes_head / (mean_ms / 1e3) / 1e9
     # DRAM bytes per launch of this kernel and workload, from the committed ncu capture
     traffic = None
@@ -407,7 +410,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "algorithmic_bytes_per_launch": bytes_head, "hops_per_query": round(hops_head, 2),
-                         "evals_per_query": round(evals_head, 1), "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)"},
+                         "evals_per_query": round(evals_head, 1), "peak_source": peak_source},
             "clocks": clocks,
         }
         if cpu:
