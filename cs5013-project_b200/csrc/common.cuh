@@ -32,7 +32,6 @@ constexpr uint32_t kStatusTimeout  = 4u;  // a bounded device wait gave up
 // words of the index's device status array
 constexpr uint32_t kWordStatus   = 0;  // kStatus* bits, cleared by vann_sync
 constexpr uint32_t kWordU8Inexact = 1;  // set when a row was not an integer in [0, 255]
-constexpr uint32_t kWordOverflow  = 2;  // nodes handed from prune_tc_kernel to prune_kernel
 constexpr uint32_t kWordPruned    = 4;  // 2 x u64: nodes pruned by prune_tc_kernel, by prune_kernel
 
 // ---------------------------------------------------------------- bloom hashes
