@@ -123,14 +123,19 @@ struct StoreU8 {
     }
 };
 
-// lanes per row and chunks per lane of store S in dimension class DC
+// Lanes per row (kT), 16-byte chunks per lane (kCPL) and rows per lane (kM) of
+// store S in dimension class DC.  Integer rows of 128 bytes take 4 lanes of 2
+// chunks and 4 rows each: half the row-id, address and cross-lane reduction work
+// of 8 lanes of one chunk, for the same 32 rows per gather round.
 template <typename S, int DC>
 struct Layout {
-    static constexpr int kChunks128 = S::kLanes128;
-    static constexpr int kT   = (S::kLanes128 << DC) < 32 ? (S::kLanes128 << DC) : 32;
-    static constexpr int kCPL = (S::kLanes128 << DC) / kT;
-    static constexpr int kP   = 32 / kT;          // rows per warp load
-    static constexpr int kG   = S::kM * kP;       // rows per gather round
+    static constexpr int  kChunks = S::kLanes128 << DC;
+    static constexpr bool kNarrow = S::kInt && kChunks == 8;
+    static constexpr int  kT   = kNarrow ? 4 : (kChunks < 32 ? kChunks : 32);
+    static constexpr int  kCPL = kChunks / kT;
+    static constexpr int  kP   = 32 / kT;              // rows per warp load
+    static constexpr int  kM   = kNarrow ? 4 : S::kM;  // rows per lane per round
+    static constexpr int  kG   = kM * kP;              // rows per gather round
 };
 
 __device__ __forceinline__ uint4 load16(const void* base, uint64_t row_bytes, uint64_t row, uint32_t k) {
@@ -224,22 +229,25 @@ template <typename S, int DC>
 __device__ __forceinline__ uint32_t round_row_of_lane(uint32_t lane) {
     using Ly        = Layout<S, DC>;
     const uint32_t t = lane % Ly::kT, g = lane / Ly::kT;
-    return (t / (Ly::kT / S::kM)) * Ly::kP + g;
+    return (t / (Ly::kT / Ly::kM)) * Ly::kP + g;
 }
 template <typename S, int DC>
 __device__ __forceinline__ bool round_writer(uint32_t lane) {
     using Ly = Layout<S, DC>;
-    return (lane % (Ly::kT / S::kM)) == 0u;
+    return (lane % (Ly::kT / Ly::kM)) == 0u;
 }
 
 // Squared L2 from the query to rows ids(0) .. ids(cnt-1), cnt <= kG (uniform
 // across the warp).  All loads are issued before any arithmetic.  The result
 // for row round_row_of_lane(lane) is returned in the lanes where round_writer.
+// Integer stores skip the row slots m with no row in any lane (m * kP >= cnt,
+// a partial round): no loads and no arithmetic.  (The same branch around the
+// float stores' loads costs more than it saves.)
 template <typename S, int DC, typename IdFn>
 __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* base, const float* scale,
                                             IdFn ids, int cnt, uint32_t D, uint32_t lane) {
     using Ly                 = Layout<S, DC>;
-    constexpr int  M         = S::kM;
+    constexpr int  M         = Ly::kM;
     const uint32_t chunks    = D / S::kElems;
     const uint64_t row_bytes = (uint64_t)D * (16 / S::kElems);
     const uint32_t t         = lane % Ly::kT;
@@ -248,6 +256,12 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
     float          sc[M];
 #pragma unroll
     for (int m = 0; m < M; ++m) {
+        if (S::kInt && m * Ly::kP >= cnt) {
+#pragma unroll
+            for (int c = 0; c < Ly::kCPL; ++c) x[m][c] = make_uint4(0u, 0u, 0u, 0u);
+            sc[m] = 0.f;
+            continue;
+        }
         const int r     = m * Ly::kP + (int)g;
         const bool valid = r < cnt;
         uint32_t   id    = valid ? ids(r) : 0u;
@@ -264,6 +278,8 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
             int v[M];
 #pragma unroll
             for (int m = 0; m < M; ++m) {
+                v[m] = 0;
+                if (m * Ly::kP >= cnt) continue;
                 unsigned xx = 0u, qx = 0u;
 #pragma unroll
                 for (int c = 0; c < Ly::kCPL; ++c) {

@@ -1153,7 +1153,7 @@ vann_status vann_consolidate(vann_index* h, void* stream) {
             a.vecs_f32 = h->vecs;
             a.deg = h->deg;
             a.adj = h->adj;
-        a.adj_h = h->adj_h;
+            a.adj_h = h->adj_h;
             a.R = R;
             a.tomb = h->tomb;
             a.queries = qv;
