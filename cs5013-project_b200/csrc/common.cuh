@@ -329,6 +329,34 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
     return group_reduce<M, Ly::kT, float>(v, lane);
 }
 
+// ---------------------------------------------------------------- launches
+// Blocks per SM of a launch, and the shared-memory carveout set to the smallest
+// one that still holds them.  The rest of the SM's unified L1/shared memory
+// stays L1, where register spills and the rows and lists that several warps
+// touch are cached.
+template <typename K>
+inline cudaError_t fit_carveout(K kern, int threads, size_t smem, int* per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern, threads, smem);
+    if (e != cudaSuccess || *per_sm < 1) return e;
+    int dev = 0, cap = 0, rsv = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&cap, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev)) != cudaSuccess) return e;
+    const size_t need = (size_t)*per_sm * (smem + (size_t)rsv);
+    const int    pct  = (int)((need * 100 + (size_t)cap - 1) / (size_t)cap);
+    if (pct >= 100) return cudaSuccess;
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct)) != cudaSuccess) return e;
+    int check = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&check, kern, threads, smem)) != cudaSuccess) return e;
+    if (check < *per_sm)  // a coarser carveout step than asked for: keep all of it
+        return cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxShared);
+    return cudaSuccess;
+}
+
 // ---------------------------------------------------------------- keys
 // Non-negative float distances order like their bit patterns.
 __device__ __forceinline__ uint64_t make_key(float d, uint32_t lo) {

@@ -223,10 +223,8 @@ cudaError_t launch_prune_rev(const PruneArgs& a, uint32_t* out_list, uint32_t* o
     auto         kern  = a.D <= 128 ? prune_rev_kernel<0> : prune_rev_kernel<1>;
     cudaError_t  e     = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
-    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e          = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
+    e          = fit_carveout(kern, warps * 32, smem, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     uint64_t grid = (uint64_t)per_sm * num_sms;

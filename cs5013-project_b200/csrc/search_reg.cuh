@@ -362,11 +362,8 @@ static cudaError_t launch_rw(const SearchArgs& a, int num_sms, cudaStream_t st) 
     auto       kern  = search_kernel_rw<S, DC, SPL, LREG, MINB>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             (int)cudaSharedmemCarveoutMaxShared);
-    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
+    e = fit_carveout(kern, warps * 32, smem, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     uint64_t need = (a.nq + warps - 1) / warps;
