@@ -41,6 +41,10 @@ sys.path.insert(0, os.path.join(ROOT, "cs5013-project_b200"))
 sys.path.insert(0, ROOT)
 
 N_BASE, N_QUERY, DIM, R, L_BUILD, ALPHA, BATCH, K = 1_000_000, 10_000, 128, 64, 100, 1.2, 10_000, 10
+# the reference CUDA search's compile-time configuration (vamana/include/constants.cuh:7-13):
+# 10,000 records of D=128, R=64, worklist L=199, entry (medoid) 5000
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_vamana")
+REF_N, REF_R, REF_L, REF_ENTRY, REF_NQ = 10_000, 64, 199, 5000, 10_000
 L_SWEEP = [32, 40, 48, 56, 64, 80, 96, 128, 160, 192, 256]
 TARGET = 0.95
 
@@ -151,6 +155,47 @@ def build_index(torch, vann, base_d, dev):
     idx.build(base_d, batch=BATCH, seed=2024)
     torch.cuda.synchronize()
     return idx, time.time() - t0
+
+
+def ref_config_index(torch, vann, dev):
+    """The graph and queries of the reference GPU search's own configuration: 10,000 x
+    128 integer-valued rows (100-cluster mixture), a graph built by this engine (R=64,
+    L=100, alpha=1.2) with the entry set to 5000, and 10,000 queries."""
+    from vann import workload
+
+    base = workload.mixture(REF_N, DIM, 100, seed=1)
+    q = workload.mixture(REF_NQ, DIM, 100, seed=2)
+    built = vann.Index(DIM, REF_R, L_BUILD, ALPHA, capacity=REF_N)
+    built.build(torch.from_numpy(base).to(dev), batch=0, seed=7)
+    vecs, deg, adj = built.get_graph()
+    del built
+    idx = vann.Index(DIM, REF_R, REF_L, ALPHA, capacity=REF_N)
+    idx.set_graph(vecs, deg, adj, REF_ENTRY)
+    return idx, q
+
+
+def at_ref_config(torch, vann, dev, steps=5):
+    """This engine at the reference GPU search's configuration: one vann_search call
+    over the 10,000 device-resident queries at L=199 with the reference's batch-index
+    skip, timed by wall clock around the call and a synchronize, as the reference's
+    greedySearch is (it returns only after its last hop)."""
+    idx, q = ref_config_index(torch, vann, dev)
+    qd = torch.from_numpy(q).to(dev)
+    out = (torch.empty((REF_NQ, K), dtype=torch.int32, device=dev),
+           torch.empty((REF_NQ, K), dtype=torch.float32, device=dev))
+    run = lambda: idx.search(qd, k=K, L=REF_L, quirks=vann.QUIRK_SKIP_BATCH_INDEX, out=out)
+    for _ in range(3):
+        run()
+    ms = []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        run()
+        torch.cuda.synchronize()
+        ms.append(1e3 * (time.perf_counter() - t0))
+    return {"workload": f"{REF_N}x{DIM} graph R={REF_R} (built by this engine, entry {REF_ENTRY}); "
+                        f"{REF_NQ} device-resident queries; L={REF_L}; batch-index skip",
+            "qps": round(REF_NQ / (statistics.mean(ms) / 1e3), 1), "ms_per_call": [round(t, 3) for t in ms]}
 
 
 def max_over_ranks(torch, dist, values, device):
@@ -415,6 +460,9 @@ def main():
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if world == 1 and not args.only and not args.profile:
+            # beside the reference arm's "reference_gpu": the same graph, queries and L
+            line["at_reference_gpu_config"] = at_ref_config(torch, vann, dev)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -502,8 +550,34 @@ def main_reference():
                          "sample": f"{sample} queries per step, oracle/vann_oracle.c GreedySearch"},
         "e2e": {"value": round(qps, 1), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if os.path.exists(REF_BIN):
+        line["reference_gpu"] = reference_gpu(torch, vann, dev)
     print(json.dumps(line), flush=True)
     return 0
+
+
+def reference_gpu(torch, vann, dev, reps=3):
+    """The reference's own CUDA greedySearch (search.cuh:226-367, compiled for sm_100a by
+    `make -C oracle ref`) at its compile-time configuration, over the graph and queries
+    of ref_config_index; wall time per call as its driver measures it."""
+    import tempfile
+
+    idx, q = ref_config_index(torch, vann, dev)
+    with tempfile.TemporaryDirectory() as td:
+        gp, qp = os.path.join(td, "graph.bin"), os.path.join(td, "q.f32")
+        idx.save_graph(gp)
+        q.tofile(qp)
+        del idx
+        r = subprocess.run([REF_BIN, "time", gp, qp, str(REF_NQ), str(reps)], capture_output=True, text=True,
+                           timeout=600)
+    times = [ln for ln in r.stdout.splitlines() if ln.startswith("REFTIME")]
+    if r.returncode != 0 or not times:
+        return {"unavailable": f"ref_vamana exited {r.returncode}: {r.stderr.strip()[-200:]}"}
+    ms = [float(x) for x in times[-1].split()[1:]]
+    return {"kind": "reference CUDA greedySearch (oracle/_ref/ref_vamana, sm_100a)",
+            "workload": f"{REF_N}x{DIM} graph R={REF_R} (built by this engine, entry {REF_ENTRY}); "
+                        f"{REF_NQ} device-resident queries; L={REF_L}",
+            "qps": round(REF_NQ / (statistics.mean(ms) / 1e3), 1), "ms_per_call": ms}
 
 
 def gt_live(torch, vec_by_id, live_ids_d, q_d, k):
