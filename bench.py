@@ -11,7 +11,8 @@ point is the smallest L whose recall@10 >= 0.95.
 
 A step is one batched search of the 10,000 queries.  `value` is the queries/s of
 the fastest reduced-precision form at recall@10 >= 0.95 (uint8 or BF16 traversal
-copies, or FP8 traversal with an exact FP32 rerank), device time with CUDA events
+copies, FP8 traversal with an exact FP32 rerank, or the uint8 copy searched two
+parents per hop), device time with CUDA events
 on the launching stream, L2 flushed before every step.  `e2e` repeats it through
 the public C ABI with pinned host buffers: each step copies the queries in and the
 ids/distances out inside the timed region, the L2 flushed before every search.
@@ -272,16 +273,21 @@ def main():
 
     # ---- sweep
     sweep = {}
-    forms = [("f32", False), ("bf16", False), ("u8", False), ("fp8", True)]
+    # (name, traversal copy, exact FP32 rerank, parents per hop); beam 2 is the batched
+    # two-parents-per-hop form, swept only where its register worklist applies (L <= 64)
+    forms = [("f32", "f32", False, 1), ("bf16", "bf16", False, 1), ("u8", "u8", False, 1),
+             ("fp8+rerank", "fp8", True, 1), ("u8/beam2", "u8", False, 2)]
     sweep_L = L_SWEEP
     if args.only:
         oname, oL = args.only.split("@")
-        forms = [f for f in forms if f[0] + ("+rerank" if f[1] else "") == oname]
+        forms = [f for f in forms if f[0] == oname]
         sweep_L = [int(oL)]
-    for store, rr in forms:
-        name = store + ("+rerank" if rr else "")
+    form_of = {f[0]: f for f in forms}
+    for name, store, rr, beam in forms:
         for L in sweep_L:
-            ids, _ = idx.search(q_d, k=K, L=L, store=store, rerank=rr)
+            if beam > 1 and L > 64:
+                continue
+            ids, _ = idx.search(q_d, k=K, L=L, store=store, rerank=rr, beam=beam)
             torch.cuda.synchronize()
             sweep.setdefault(name, []).append((L, recall(torch, ids, gt)))
     idx.sync()
@@ -294,9 +300,8 @@ def main():
         return sweep[name][-1][0]
 
     tune_ms = {}
-    for store, rr in forms:
-        name = store + ("+rerank" if rr else "")
-        tune_ms[name] = idx.autotune(q_d, k=K, L=op_point0(name), store=store, rerank=rr)
+    for name, store, rr, beam in forms:
+        tune_ms[name] = idx.autotune(q_d, k=K, L=op_point0(name), store=store, rerank=rr, beam=beam)
 
     def op_point(name):
         for L, r in sweep[name]:
@@ -309,10 +314,9 @@ def main():
     results = {}
     steps, warm = (3, 1) if args.profile else (args.steps, args.warmup)
     with Clocks(local) as clk:
-        for store, rr in forms:
-            name = store + ("+rerank" if rr else "")
+        for name, store, rr, beam in forms:
             L, r = op_point(name)
-            fn = lambda s=store, rr=rr, L=L: idx.search(q_d, k=K, L=L, store=s, rerank=rr, out=out)
+            fn = lambda s=store, rr=rr, L=L, b=beam: idx.search(q_d, k=K, L=L, store=s, rerank=rr, out=out, beam=b)
             t = time_steps(torch, fn, steps, warm, flush, dist)
             results[name] = {"L": L, "recall": r, "ms": t}
     clocks = clk.summary()
@@ -330,9 +334,8 @@ def main():
 
     # work counters of the headline and FP32 forms (algorithmic bytes)
     def counted_bytes(name):
-        store = name.split("+")[0]
-        rr = name.endswith("+rerank")
-        _, _, st = idx.search_stats(q_d, k=K, L=results[name]["L"], store=store, rerank=rr)
+        _, store, rr, beam = form_of[name]
+        _, _, st = idx.search_stats(q_d, k=K, L=results[name]["L"], store=store, rerank=rr, beam=beam)
         st = st.cpu().numpy().astype(np.int64)
         hops, evals, adjw = st[0], st[1], st[2]
         s = {"f32": 4, "bf16": 2, "u8": 1, "fp8": 1}[store]
@@ -369,8 +372,7 @@ def main():
     # double-buffered so one step's copies overlap its neighbours' searches (an
     # upload stream and a download stream beside the compute stream), as a
     # serving pipeline would run.
-    hs = head.split("+")[0]
-    hrr = head.endswith("+rerank")
+    _, hs, hrr, hbeam = form_of[head]
     h_q = torch.from_numpy(q).pin_memory()
     s_comp = torch.cuda.current_stream()
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
@@ -396,7 +398,7 @@ def main():
                 s_comp.wait_event(ev_out[bsel])  # the download of this buffer's last results
             with torch.cuda.stream(s_comp):
                 flush.zero_()  # L2 flushed before every search, as in the device-timed loop
-            idx.search(qbuf[bsel], k=K, L=hr["L"], store=hs, rerank=hrr, out=obuf[bsel], stream=s_comp)
+            idx.search(qbuf[bsel], k=K, L=hr["L"], store=hs, rerank=hrr, out=obuf[bsel], stream=s_comp, beam=hbeam)
             ev_done[bsel].record(s_comp)
             with torch.cuda.stream(s_out):
                 s_out.wait_event(ev_done[bsel])

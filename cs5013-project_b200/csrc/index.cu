@@ -131,11 +131,12 @@ struct vann_index {
     // per-query L / k arrays of the vann_search_uneven call in progress
     const uint32_t* pending_Lq = nullptr;
     const uint32_t* pending_kq = nullptr;
-    // autotuned search variant per (store, rerank, L)
-    std::map<std::tuple<uint32_t, uint32_t, uint32_t>, int> tuned;
+    // autotuned search variant per (store, rerank, beam, L)
+    std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>, int> tuned;
 
+    static uint32_t beam_of(const vann_search_params& sp) { return sp.beam == 2 ? 2u : 1u; }
     int variant_for(const vann_search_params& sp) const {
-        auto it = tuned.find(std::make_tuple(sp.store, sp.rerank ? 1u : 0u, sp.L));
+        auto it = tuned.find(std::make_tuple(sp.store, sp.rerank ? 1u : 0u, beam_of(sp), sp.L));
         return it == tuned.end() ? 0 : it->second;
     }
 
@@ -821,9 +822,13 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
                  "need 1 <= k <= L <= 1024");
         VREQUIRE(sp->store < 4 && h->store[sp->store] != nullptr, VANN_ERR_UNSUPPORTED,
                  "requested store was not enabled at create");
+        VREQUIRE(sp->beam <= 2, VANN_ERR_INVALID, "beam must be 0, 1 or 2");
+        VREQUIRE(sp->beam < 2 || (sp->L <= 64 && h->p.dim <= 128 && h->p.degree <= 64), VANN_ERR_UNSUPPORTED,
+                 "beam 2 needs L <= 64, dim <= 128 and degree <= 64");
         VREQUIRE(h->size > 0 && h->entry < h->size, VANN_ERR_STATE, "index is empty");
         if (nq == 0) return;
         vann::SearchArgs a{};
+        a.beam  = vann_index::beam_of(*sp);
         a.store = h->store[sp->store];
         a.scale = h->fp8_scale;
         a.vecs_f32 = h->vecs;
@@ -938,7 +943,7 @@ vann_status vann_autotune(vann_index* h, const float* d_queries, uint64_t nq, co
         cudaEvent_t e0, e1;
         VCHECK(cudaEventCreate(&e0));
         VCHECK(cudaEventCreate(&e1));
-        const auto key = std::make_tuple(sp->store, sp->rerank ? 1u : 0u, sp->L);
+        const auto key = std::make_tuple(sp->store, sp->rerank ? 1u : 0u, vann_index::beam_of(*sp), sp->L);
         int   best = 0;
         float best_ms = 1e30f;
         for (int v = 0; v < vann::search_variants(); ++v) {

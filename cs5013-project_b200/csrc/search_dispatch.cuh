@@ -11,32 +11,32 @@ namespace vann {
 // exist for the common shape (D <= 128, R <= 64); the autotuner picks one.
 constexpr int kSearchVariants = 7;
 
+template <typename S, int DC, int SPL, int LREG, int BEAM>
+static cudaError_t launch_rw_v(const SearchArgs& a, int variant, int sms, cudaStream_t st) {
+    switch (variant) {
+        case 1: return launch_rw<S, DC, SPL, LREG, 4, BEAM>(a, sms, st);
+        case 2: return launch_rw<S, DC, SPL, LREG, 5, BEAM>(a, sms, st);
+        case 3: return launch_rw<S, DC, SPL, LREG, 7, BEAM>(a, sms, st);
+        case 4: return launch_rw<S, DC, SPL, LREG, 8, BEAM>(a, sms, st);
+        case 5: return launch_rw<S, DC, SPL, LREG, 9, BEAM>(a, sms, st);
+        case 6: return launch_rw<S, DC, SPL, LREG, 10, BEAM>(a, sms, st);
+        default: return launch_rw<S, DC, SPL, LREG, 6, BEAM>(a, sms, st);
+    }
+}
+
 template <typename S, int DC, int SPL>
 static cudaError_t launch_v(const SearchArgs& a, int variant, int sms, cudaStream_t st) {
     if constexpr (DC == 0 && SPL <= 2) {
-        // worklist in registers for L <= 64
-        if (a.L <= 32) {
-            switch (variant) {
-                case 1: return launch_rw<S, DC, SPL, 1, 4>(a, sms, st);
-                case 2: return launch_rw<S, DC, SPL, 1, 5>(a, sms, st);
-                case 3: return launch_rw<S, DC, SPL, 1, 7>(a, sms, st);
-                case 4: return launch_rw<S, DC, SPL, 1, 8>(a, sms, st);
-                case 5: return launch_rw<S, DC, SPL, 1, 9>(a, sms, st);
-                case 6: return launch_rw<S, DC, SPL, 1, 10>(a, sms, st);
-                default: return launch_rw<S, DC, SPL, 1, 6>(a, sms, st);
-            }
-        }
-        if (a.L <= 64) {
-            switch (variant) {
-                case 1: return launch_rw<S, DC, SPL, 2, 4>(a, sms, st);
-                case 2: return launch_rw<S, DC, SPL, 2, 5>(a, sms, st);
-                case 3: return launch_rw<S, DC, SPL, 2, 7>(a, sms, st);
-                case 4: return launch_rw<S, DC, SPL, 2, 8>(a, sms, st);
-                case 5: return launch_rw<S, DC, SPL, 2, 9>(a, sms, st);
-                case 6: return launch_rw<S, DC, SPL, 2, 10>(a, sms, st);
-                default: return launch_rw<S, DC, SPL, 2, 6>(a, sms, st);
-            }
-        }
+        // worklist in registers for L <= 64; two parents per hop only here
+        if (a.L <= 32)
+            return a.beam == 2 ? launch_rw_v<S, DC, SPL, 1, 2>(a, variant, sms, st)
+                               : launch_rw_v<S, DC, SPL, 1, 1>(a, variant, sms, st);
+        if (a.L <= 64)
+            return a.beam == 2 ? launch_rw_v<S, DC, SPL, 2, 2>(a, variant, sms, st)
+                               : launch_rw_v<S, DC, SPL, 2, 1>(a, variant, sms, st);
+    }
+    if (a.beam == 2) return cudaErrorInvalidValue;
+    if constexpr (DC == 0 && SPL <= 2) {
         switch (variant) {
             case 1: return launch_t<S, DC, SPL, 4>(a, sms, st);
             case 2: return launch_t<S, DC, SPL, 5>(a, sms, st);

@@ -10,6 +10,12 @@
 // (mergeIntoWorklist, search.cuh:140-223).  A merge is a half-cleaner between
 // the worklist and the reversed sorted candidates followed by a bitonic merge
 // network; the next parent is one ballot.
+//
+// BEAM = 2 is a batched form beside the reference's algorithm (not a parity
+// form): each hop expands the first two unvisited entries together, so a query
+// takes about half the hops, each with two lists in flight and fuller gather
+// rounds.  The second list is filtered after the first one's marks, and the kept
+// candidates are sorted and merged in batches of up to 64.
 #pragma once
 #include "search_impl.cuh"
 
@@ -69,14 +75,15 @@ __device__ __forceinline__ void reg_merge(uint64_t (&wk)[LREG], uint32_t (&wp)[L
     }
 }
 
-template <typename S, int DC, int SPL, int LREG, int MINB>
+template <typename S, int DC, int SPL, int LREG, int MINB, int BEAM>
 __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
+    static_assert(BEAM == 1 || BEAM == 2, "one or two parents per hop");
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int   G     = Layout<S, DC>::kG;
-    constexpr int   N     = 32 * LREG;
+    constexpr int   NS    = BEAM * SPL;  // neighbour slots per lane in one hop
     const uint32_t  lane  = threadIdx.x & 31u;
     const uint32_t  wib   = threadIdx.x >> 5;
-    const RegLayout lay   = RegLayout::make(SPL * 32);
+    const RegLayout lay   = RegLayout::make(NS * 32);
     unsigned char*  base  = smem + (size_t)wib * lay.bytes;
     uint32_t*       bloom = reinterpret_cast<uint32_t*>(base);
     uint32_t*       nb_id = reinterpret_cast<uint32_t*>(base + 5008);
@@ -118,21 +125,30 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
             wk[0] = make_key(d0, 0u);
             wp[0] = entry | kVisitedBit;
         }
-        uint32_t n = 1, seq = 1, parent = entry, hops = 0, nv = 0, evals = 1, adjw = 0;
-        float    pd = d0;
-        uint32_t nid[SPL], hp[SPL], dg;
-        auto     fetch_row = [&](uint32_t node) {
-            const uint32_t* row  = a.adj + (uint64_t)node * R;
-            const uint32_t* rowh = a.adj_h + (uint64_t)node * R;
+        uint32_t n = 1, seq = 1, hops = 0, nv = 0, evals = 1, adjw = 0, np = 1;
+        uint32_t par[BEAM];
+        float    pd[BEAM];
+        par[0] = entry;
+        pd[0]  = d0;
+        // the parents' degrees, adjacency rows and filter slots, all in one round trip
+        uint32_t nid[BEAM][SPL], hp[BEAM][SPL], dg[BEAM];
+        auto     fetch_rows = [&]() {
 #pragma unroll
-            for (int s = 0; s < SPL; ++s) {
-                uint32_t j = (uint32_t)s * 32u + lane;
-                nid[s]     = j < R ? __ldg(row + j) : 0u;
-                hp[s]      = j < R ? __ldg(rowh + j) : 0u;
+            for (int b = 0; b < BEAM; ++b) {
+                const bool      live = (uint32_t)b < np;
+                const uint32_t  node = live ? par[b] : 0u;
+                const uint32_t* row  = a.adj + (uint64_t)node * R;
+                const uint32_t* rowh = a.adj_h + (uint64_t)node * R;
+#pragma unroll
+                for (int s = 0; s < SPL; ++s) {
+                    uint32_t j = (uint32_t)s * 32u + lane;
+                    nid[b][s]  = live && j < R ? __ldg(row + j) : 0u;
+                    hp[b][s]   = live && j < R ? __ldg(rowh + j) : 0u;
+                }
+                dg[b] = live ? __ldg(a.deg + node) : 0u;
             }
-            dg = __ldg(a.deg + node);
         };
-        fetch_row(parent);
+        fetch_rows();
 
         for (;;) {
             if (hops >= a.max_hops) {
@@ -140,44 +156,49 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
                 break;
             }
             ++hops;
-            if (a.vis_ids != nullptr && nv < a.max_visited) {
-                if (lane == 0) {
-                    a.vis_ids[(uint64_t)q * a.max_visited + nv] = parent;
-                    a.vis_d[(uint64_t)q * a.max_visited + nv]   = pd;
-                }
-                ++nv;
-            }
-            dg = dg < R ? dg : R;
-            adjw += dg;
-
-            // filterNeighbors: snapshot check of every slot, then mark
-            bool pass[SPL];
-#pragma unroll
-            for (int s = 0; s < SPL; ++s) {
-                uint32_t j  = (uint32_t)s * 32u + lane;
-                bool     ok = j < dg;
-                if (ok && a.tomb != nullptr) ok = !((__ldg(a.tomb + (nid[s] >> 5)) >> (nid[s] & 31u)) & 1u);
-                if (ok && nid[s] == skip) ok = false;
-                if (ok) {
-                    uint32_t h1 = hp[s] >> 16, h2 = hp[s] & 0xffffu;
-                    ok = !(((bloom[h1 >> 5] >> (h1 & 31u)) & 1u) && ((bloom[h2 >> 5] >> (h2 & 31u)) & 1u));
-                }
-                pass[s] = ok;
-            }
-            __syncwarp();
             uint32_t cnt = 0;
 #pragma unroll
-            for (int s = 0; s < SPL; ++s) {
-                if (pass[s]) {
-                    uint32_t h1 = hp[s] >> 16, h2 = hp[s] & 0xffffu;
-                    atomicOr(&bloom[h1 >> 5], 1u << (h1 & 31u));
-                    atomicOr(&bloom[h2 >> 5], 1u << (h2 & 31u));
+            for (int b = 0; b < BEAM; ++b) {
+                if ((uint32_t)b >= np) break;
+                if (a.vis_ids != nullptr && nv < a.max_visited) {
+                    if (lane == 0) {
+                        a.vis_ids[(uint64_t)q * a.max_visited + nv] = par[b];
+                        a.vis_d[(uint64_t)q * a.max_visited + nv]   = pd[b];
+                    }
+                    ++nv;
                 }
-                uint32_t m = __ballot_sync(0xffffffffu, pass[s]);
-                if (pass[s]) nb_id[cnt + __popc(m & ((1u << lane) - 1u))] = nid[s];
-                cnt += __popc(m);
+                const uint32_t dgb = dg[b] < R ? dg[b] : R;
+                adjw += dgb;
+
+                // filterNeighbors: snapshot check of every slot of the list, then mark
+                bool pass[SPL];
+#pragma unroll
+                for (int s = 0; s < SPL; ++s) {
+                    const uint32_t j  = (uint32_t)s * 32u + lane;
+                    const uint32_t id = nid[b][s];
+                    bool           ok = j < dgb;
+                    if (ok && a.tomb != nullptr) ok = !((__ldg(a.tomb + (id >> 5)) >> (id & 31u)) & 1u);
+                    if (ok && id == skip) ok = false;
+                    if (ok) {
+                        uint32_t h1 = hp[b][s] >> 16, h2 = hp[b][s] & 0xffffu;
+                        ok = !(((bloom[h1 >> 5] >> (h1 & 31u)) & 1u) && ((bloom[h2 >> 5] >> (h2 & 31u)) & 1u));
+                    }
+                    pass[s] = ok;
+                }
+                __syncwarp();
+#pragma unroll
+                for (int s = 0; s < SPL; ++s) {
+                    if (pass[s]) {
+                        uint32_t h1 = hp[b][s] >> 16, h2 = hp[b][s] & 0xffffu;
+                        atomicOr(&bloom[h1 >> 5], 1u << (h1 & 31u));
+                        atomicOr(&bloom[h2 >> 5], 1u << (h2 & 31u));
+                    }
+                    uint32_t m = __ballot_sync(0xffffffffu, pass[s]);
+                    if (pass[s]) nb_id[cnt + __popc(m & ((1u << lane) - 1u))] = nid[b][s];
+                    cnt += __popc(m);
+                }
+                __syncwarp();
             }
-            __syncwarp();
             evals += cnt;
 
             for (uint32_t g0 = 0; g0 < cnt; g0 += G) {
@@ -199,10 +220,10 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
                     if (r == last / 32) mine = wk[r];
                 tail = key_dist(__shfl_sync(0xffffffffu, mine, last % 32));
             }
-            uint64_t ckey[SPL];
-            bool     keep[SPL];
+            uint64_t ckey[NS];
+            bool     keep[NS];
 #pragma unroll
-            for (int s = 0; s < SPL; ++s) {
+            for (int s = 0; s < NS; ++s) {
                 uint32_t j = (uint32_t)s * 32u + lane;
                 keep[s]    = false;
                 ckey[s]    = kSentinel;
@@ -215,28 +236,31 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
             __syncwarp();
             uint32_t kc = 0;
 #pragma unroll
-            for (int s = 0; s < SPL; ++s) {
+            for (int s = 0; s < NS; ++s) {
                 uint32_t m = __ballot_sync(0xffffffffu, keep[s]);
                 if (keep[s]) nb_key[kc + __popc(m & ((1u << lane) - 1u))] = ckey[s];
                 kc += __popc(m);
             }
             __syncwarp();
 
-            if (kc > 0) {
+            // at most 64 kept candidates per batch (one batch unless BEAM = 2)
+            for (uint32_t b0 = 0; b0 < kc; b0 += 64u) {
+                const uint32_t  bc = min(64u, kc - b0);
+                const uint64_t* bk = nb_key + b0;
                 // sort the kept candidates by (distance, id); only the best N can enter
                 uint64_t ck[LREG];
                 uint32_t cp[LREG];
-                if (kc <= 32) {
-                    uint64_t k1[1] = {lane < kc ? nb_key[lane] : kSentinel};
+                if (bc <= 32) {
+                    uint64_t k1[1] = {lane < bc ? bk[lane] : kSentinel};
                     uint32_t n2    = 1;
-                    while (n2 < kc) n2 <<= 1;
+                    while (n2 < bc) n2 <<= 1;
                     if (n2 > 1) warp_bitonic_sort<1>(k1, lane, n2);
                     ck[0] = k1[0];
                     if constexpr (LREG == 2) ck[1] = kSentinel;
                 } else {
                     uint64_t k2[2];
-                    k2[0] = nb_key[lane];
-                    k2[1] = lane + 32u < kc ? nb_key[lane + 32u] : kSentinel;
+                    k2[0] = bk[lane];
+                    k2[1] = lane + 32u < bc ? bk[lane + 32u] : kSentinel;
                     warp_bitonic_sort<2>(k2, lane, 64u);
                     ck[0] = k2[0];
                     if constexpr (LREG == 2) ck[1] = k2[1];
@@ -245,7 +269,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
 #pragma unroll
                 for (int r = 0; r < LREG; ++r) {
                     uint32_t e = (uint32_t)r * 32u + lane;
-                    if (ck[r] != kSentinel && e < kc) {
+                    if (ck[r] != kSentinel && e < bc) {
                         cp[r] = (uint32_t)ck[r];
                         ck[r] = (ck[r] & 0xffffffff00000000ull) | (uint64_t)(seq + e);
                     } else {
@@ -253,9 +277,9 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
                         ck[r] = kSentinel;
                     }
                 }
-                seq += kc;
+                seq += bc;
                 reg_merge<LREG>(wk, wp, ck, cp, lane);
-                n = min(n + kc, L);
+                n = min(n + bc, L);
 #pragma unroll
                 for (int r = 0; r < LREG; ++r) {
                     if ((uint32_t)r * 32u + lane >= L) {  // truncate to L
@@ -266,34 +290,56 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
             }
             __syncwarp();
 
-            // next parent: first unvisited entry
-            int found_r = -1, found_l = 0;
+            // next parents: the first BEAM unvisited entries, in list order
+            int      fr[BEAM], fl[BEAM];
+            uint32_t got = 0;
+#pragma unroll
+            for (int b = 0; b < BEAM; ++b) {
+                fr[b] = -1;
+                fl[b] = 0;
+            }
 #pragma unroll
             for (int r = 0; r < LREG; ++r) {
                 uint32_t m = __ballot_sync(0xffffffffu, wk[r] != kSentinel && !(wp[r] & kVisitedBit));
-                if (found_r < 0 && m) {
-                    found_r = r;
-                    found_l = __ffs(m) - 1;
+#pragma unroll
+                for (int b = 0; b < BEAM; ++b) {
+                    if (m != 0u && got < (uint32_t)BEAM) {
+                        const int l = __ffs(m) - 1;
+                        m &= m - 1u;
+                        if (got == 0u) {
+                            fr[0] = r;
+                            fl[0] = l;
+                        } else {
+                            fr[BEAM - 1] = r;
+                            fl[BEAM - 1] = l;
+                        }
+                        ++got;
+                    }
                 }
             }
-            if (found_r < 0) break;
-            uint32_t pk_lo = 0;
-            uint64_t pkey  = 0;
+            if (got == 0u) break;
+            np = got;
 #pragma unroll
-            for (int r = 0; r < LREG; ++r) {
-                uint32_t p  = __shfl_sync(0xffffffffu, wp[r], found_l);
-                uint64_t kk = __shfl_sync(0xffffffffu, wk[r], found_l);
-                if (r == found_r) {
-                    pk_lo = p;
-                    pkey  = kk;
+            for (int b = 0; b < BEAM; ++b) {
+                if (fr[b] < 0) continue;
+                uint32_t pk_lo = 0;
+                uint64_t pkey  = 0;
+#pragma unroll
+                for (int r = 0; r < LREG; ++r) {
+                    uint32_t p  = __shfl_sync(0xffffffffu, wp[r], fl[b]);
+                    uint64_t kk = __shfl_sync(0xffffffffu, wk[r], fl[b]);
+                    if (r == fr[b]) {
+                        pk_lo = p;
+                        pkey  = kk;
+                    }
                 }
-            }
 #pragma unroll
-            for (int r = 0; r < LREG; ++r)
-                if (r == found_r && lane == (uint32_t)found_l) wp[r] |= kVisitedBit;
-            parent = pk_lo & ~kVisitedBit;
-            pd     = key_dist(pkey);
-            fetch_row(parent);
+                for (int r = 0; r < LREG; ++r)
+                    if (r == fr[b] && lane == (uint32_t)fl[b]) wp[r] |= kVisitedBit;
+                par[b] = pk_lo & ~kVisitedBit;
+                pd[b]  = key_dist(pkey);
+            }
+            fetch_rows();
         }
 
         // outputs
@@ -354,12 +400,12 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
     }
 }
 
-template <typename S, int DC, int SPL, int LREG, int MINB>
+template <typename S, int DC, int SPL, int LREG, int MINB, int BEAM = 1>
 static cudaError_t launch_rw(const SearchArgs& a, int num_sms, cudaStream_t st) {
-    RegLayout  lay   = RegLayout::make(SPL * 32);
+    RegLayout  lay   = RegLayout::make(BEAM * SPL * 32);
     const int  warps = 4;
     size_t     smem  = (size_t)lay.bytes * warps;
-    auto       kern  = search_kernel_rw<S, DC, SPL, LREG, MINB>;
+    auto       kern  = search_kernel_rw<S, DC, SPL, LREG, MINB, BEAM>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;

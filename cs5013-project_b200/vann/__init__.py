@@ -54,7 +54,7 @@ class Params(C.Structure):
 
 class SearchParams(C.Structure):
     _fields_ = [("L", C.c_uint32), ("k", C.c_uint32), ("store", C.c_uint32), ("rerank", C.c_uint32),
-                ("flags", C.c_uint32), ("max_hops", C.c_uint32)]
+                ("flags", C.c_uint32), ("max_hops", C.c_uint32), ("beam", C.c_uint32)]
 
 
 class Info(C.Structure):
@@ -226,7 +226,9 @@ class Index:
         _check(lib().vann_build_loaded(self._h, _stream_ptr(stream)))
 
     def search(self, queries, k: int, L: int, store: str = "f32", rerank: bool = False,
-               quirks: int = 0, max_hops: int = 0, out=None, stream=None):
+               quirks: int = 0, max_hops: int = 0, out=None, stream=None, beam: int = 1):
+        """Batched search; beam=2 expands two parents per hop (a batched form with its
+        own results; beam=1 is the reference's GreedySearch)."""
         torch = _torch()
         nq = queries.shape[0]
         if out is None:
@@ -234,7 +236,7 @@ class Index:
             dists = torch.empty((nq, k), dtype=torch.float32, device=queries.device)
         else:
             ids, dists = out
-        sp = SearchParams(L, k, STORES[store], int(rerank), quirks, max_hops)
+        sp = SearchParams(L, k, STORES[store], int(rerank), quirks, max_hops, beam)
         _check(lib().vann_search(self._h, _dev(queries, torch.float32), nq, C.byref(sp),
                                  _dev(ids, torch.int32), _dev(dists, torch.float32), _stream_ptr(stream)))
         return ids, dists
@@ -255,14 +257,14 @@ class Index:
         return ids, dists
 
     def search_stats(self, queries, k: int, L: int, store: str = "f32", rerank: bool = False,
-                     quirks: int = 0, max_hops: int = 0, stream=None):
+                     quirks: int = 0, max_hops: int = 0, stream=None, beam: int = 1):
         """search() plus per-query (hops, distance evaluations, adjacency words)."""
         torch = _torch()
         nq = queries.shape[0]
         ids = torch.empty((nq, k), dtype=torch.int32, device=queries.device)
         dists = torch.empty((nq, k), dtype=torch.float32, device=queries.device)
         st = torch.empty((3, nq), dtype=torch.int32, device=queries.device)
-        sp = SearchParams(L, k, STORES[store], int(rerank), quirks, max_hops)
+        sp = SearchParams(L, k, STORES[store], int(rerank), quirks, max_hops, beam)
         _check(lib().vann_search_stats(self._h, _dev(queries, torch.float32), nq, C.byref(sp),
                                        _dev(ids, torch.int32), _dev(dists, torch.float32),
                                        C.c_void_p(st[0].data_ptr()), C.c_void_p(st[1].data_ptr()),
@@ -270,10 +272,10 @@ class Index:
         return ids, dists, st
 
     def autotune(self, queries, k: int, L: int, store: str = "f32", rerank: bool = False, quirks: int = 0,
-                 stream=None):
-        """Pick the fastest compiled search variant for (store, rerank, L) on these queries."""
+                 stream=None, beam: int = 1):
+        """Pick the fastest compiled search variant for (store, rerank, beam, L) on these queries."""
         torch = _torch()
-        sp = SearchParams(L, k, STORES[store], int(rerank), quirks, 0)
+        sp = SearchParams(L, k, STORES[store], int(rerank), quirks, 0, beam)
         nv = lib().vann_search_variant_count()
         ms = (C.c_float * nv)()
         _check(lib().vann_autotune(self._h, _dev(queries, torch.float32), queries.shape[0], C.byref(sp),

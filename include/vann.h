@@ -71,6 +71,11 @@ typedef struct {
     uint32_t rerank;   /* 1: exact FP32 rerank of the final worklist before top-k */
     uint32_t flags;    /* VANN_QUIRK_* */
     uint32_t max_hops; /* 0 = default (1,000,000) */
+    uint32_t beam;     /* parents expanded per hop: 0 or 1 = the reference's GreedySearch
+                          (search.cuh:226-367, one parent per iteration); 2 = the first
+                          two unvisited entries together (a batched form with its own
+                          results, not the reference's; needs L <= 64, dim <= 128,
+                          degree <= 64, else VANN_ERR_UNSUPPORTED) */
 } vann_search_params;
 
 typedef struct {
