@@ -9,6 +9,7 @@
 // reach the graph in the same call.
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -53,13 +54,19 @@ void set_err(const std::string& m) { g_last_error = m; }
 struct DevBuf {
     void*  p     = nullptr;
     size_t bytes = 0;
-    void   ensure(size_t b) {
+    // Grows by at least half again, in 2 MiB steps: workspaces sized by batches of
+    // slowly rising size (edge lists, sort scratch) are then reallocated a few times
+    // instead of on every batch, and every cudaFree waits for the device.
+    void ensure(size_t b) {
         if (b <= bytes) return;
+        constexpr size_t kStep = size_t(2) << 20;
+        size_t           want  = std::max(b, bytes + bytes / 2);
+        want                   = (want + kStep - 1) / kStep * kStep;
         if (p) cudaFree(p);
         p     = nullptr;
         bytes = 0;
-        VCHECK(cudaMalloc(&p, b));
-        bytes = b;
+        VCHECK(cudaMalloc(&p, want));
+        bytes = want;
     }
     template <typename T>
     T* as() const {
