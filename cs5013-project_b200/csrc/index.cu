@@ -79,6 +79,89 @@ struct DevBuf {
     }
 };
 
+// Squared FP32 distance from every query to the entry row (its float bits).
+__global__ void entry_dist_kernel(const float* queries, uint64_t nq, uint32_t D, const float* entry_row,
+                                  uint32_t* keys) {
+    const uint64_t q    = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
+    const uint32_t lane = threadIdx.x & 31u;
+    if (q >= nq) return;
+    const float* row = queries + q * D;
+    float        s   = 0.f;
+    for (uint32_t i = lane; i < D; i += 32) {
+        const float d = row[i] - entry_row[i];
+        s             = fmaf(d, d, s);
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) keys[q] = __float_as_uint(s);
+}
+
+// One block orders the queries by distance to the entry point, farthest first, in
+// kOrderBuckets equal-width distance buckets (order within a bucket is whatever the
+// shared-memory atomics give: a schedule, not a result).  Two launches in all, where
+// a device-wide radix sort of a 10k batch takes several.
+constexpr int kOrderThreads = 1024;
+constexpr int kOrderBuckets = 1024;
+__global__ void __launch_bounds__(kOrderThreads) order_by_bucket_kernel(const uint32_t* keys, uint32_t nq,
+                                                                        uint32_t* order) {
+    __shared__ uint32_t cnt[kOrderBuckets];
+    __shared__ float    lo_w[32], hi_w[32];
+    const uint32_t t = threadIdx.x;
+    float          lo = __int_as_float(0x7f800000), hi = 0.f;
+    for (uint32_t i = t; i < nq; i += kOrderThreads) {
+        const float d = __uint_as_float(keys[i]);
+        lo = fminf(lo, d);
+        hi = fmaxf(hi, d);
+    }
+    for (int o = 16; o; o >>= 1) {
+        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((t & 31u) == 0) {
+        lo_w[t >> 5] = lo;
+        hi_w[t >> 5] = hi;
+    }
+    for (uint32_t b = t; b < kOrderBuckets; b += kOrderThreads) cnt[b] = 0;
+    __syncthreads();
+    lo = lo_w[0];
+    hi = hi_w[0];
+    for (int w = 1; w < kOrderThreads / 32; ++w) {
+        lo = fminf(lo, lo_w[w]);
+        hi = fmaxf(hi, hi_w[w]);
+    }
+    const float scale = hi > lo ? (float)kOrderBuckets / (hi - lo) : 0.f;
+    auto bucket = [&](uint32_t i) {  // 0 holds the farthest queries
+        const float x = (hi - __uint_as_float(keys[i])) * scale;
+        return x >= (float)(kOrderBuckets - 1) ? (uint32_t)(kOrderBuckets - 1) : (x > 0.f ? (uint32_t)x : 0u);
+    };
+    for (uint32_t i = t; i < nq; i += kOrderThreads) atomicAdd(&cnt[bucket(i)], 1u);
+    __syncthreads();
+    {  // exclusive prefix over the buckets: one per thread, warp scans, then the warp totals
+        static_assert(kOrderBuckets == kOrderThreads, "one bucket per thread");
+        __shared__ uint32_t wsum[32];
+        const uint32_t lane = t & 31u, w = t >> 5;
+        const uint32_t c    = cnt[t];
+        uint32_t       inc  = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= (uint32_t)o) inc += v;
+        }
+        if (lane == 31u) wsum[w] = inc;
+        __syncthreads();
+        if (w == 0) {
+            uint32_t x = wsum[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= (uint32_t)o) x += v;
+            }
+            wsum[lane] = x - wsum[lane];  // exclusive over the warps
+        }
+        __syncthreads();
+        cnt[t] = wsum[w] + inc - c;
+    }
+    __syncthreads();
+    for (uint32_t i = t; i < nq; i += kOrderThreads) order[atomicAdd(&cnt[bucket(i)], 1u)] = i;
+}
+
 __global__ void scatter_rows_kernel(const float* src, const uint32_t* ids, uint64_t n, uint32_t D,
                                     float* dst, uint32_t* deg, uint32_t* tomb) {
     uint64_t r    = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
@@ -147,6 +230,7 @@ struct vann_index {
         return it == tuned.end() ? 0 : it->second;
     }
 
+    DevBuf ord;  // search order of large batches: distance keys, then the order
     DevBuf vis_ids, vis_d, vis_n, nodes, runs, ovf, stage, s2_ids, s2_d, e_keys, e_vals, e_keys2, e_vals2, counts, offsets, cub_tmp,
         medoid_ws, gather, cand, cand_n, list_n, out_tmp;
 
@@ -164,6 +248,7 @@ struct vann_index {
         cudaFree(tomb);
         cudaFree(counters);
         cudaFree(status);
+        ord.release();
         for (DevBuf* b : {&vis_ids, &vis_d, &vis_n, &nodes, &runs, &ovf, &stage, &s2_ids, &s2_d, &e_keys, &e_vals, &e_keys2, &e_vals2,
                           &counts, &offsets, &cub_tmp, &medoid_ws, &gather, &cand, &cand_n,
                           &list_n, &out_tmp})
@@ -177,6 +262,24 @@ struct vann_index {
     }
 
     uint64_t tomb_words() const { return (p.capacity + 31) / 32; }
+
+    // Order in which the warps of a search launch take its queries, or null.  A batch
+    // that outnumbers the resident warps ends with its slowest queries: warps take
+    // the queries farthest from the entry point first, since those tend to take the
+    // most hops and, started last, would run on alone.  The order only changes which
+    // warp runs a query when, never its result.
+    const uint32_t* search_order(const float* d_queries, uint64_t nq, cudaStream_t st) {
+        if (nq <= 16ull * (uint64_t)num_sms || nq > 0x7FFFFFFFull) return nullptr;
+        ord.ensure(sizeof(uint32_t) * 2 * nq);
+        uint32_t* keys  = ord.as<uint32_t>();
+        uint32_t* order = keys + nq;
+        entry_dist_kernel<<<(unsigned)((nq + 7) / 8), 256, 0, st>>>(d_queries, nq, p.dim,
+                                                                  vecs + (uint64_t)entry * p.dim, keys);
+        VCHECK(cudaGetLastError());
+        order_by_bucket_kernel<<<1, kOrderThreads, 0, st>>>(keys, (uint32_t)nq, order);
+        VCHECK(cudaGetLastError());
+        return order;
+    }
 
     uint32_t* u8_inexact() const { return status + vann::kWordU8Inexact; }
     int       u8_state = -1;  // exactness of the uint8 copy seen by the host: -1 unknown, 0 no, 1 yes
@@ -308,6 +411,7 @@ struct vann_index {
         a.vis_d = vis_d.as<float>();
         a.vis_n = vis_n.as<uint32_t>();
         a.max_visited = MV;
+        a.order = search_order(d_q, count, st);
         a.counter = next_counter(st);
         a.status = status;
         // exact uint8 rows give the FP32 distances bit for bit from a quarter of the bytes
@@ -860,6 +964,7 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
         a.adjw_out = d_adjw;
         a.Lq = h->pending_Lq;
         a.kq = h->pending_kq;
+        a.order = h->search_order(d_queries, nq, S(stream));
         a.counter = h->next_counter(S(stream));
         a.status = h->status;
         VCHECK(vann::launch_search(a, (int)sp->store, h->num_sms, S(stream), h->variant_for(*sp)));

@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
         if (lane == 0) q = atomicAdd(a.counter, 1u);
         q = __shfl_sync(0xffffffffu, q, 0);
         if (q >= a.nq) break;
+        if (a.order != nullptr) q = __ldg(a.order + q);  // the query's index in the batch
         // per-query worklist size and result count (uneven batches), capped by the
         // launch's maximum, which sized the shared memory and the output rows
         const uint32_t L  = a.Lq != nullptr ? max(1u, min(__ldg(a.Lq + q), a.L)) : a.L;

@@ -175,3 +175,24 @@ def test_uneven_batch_equals_separate_launches(oracle, vann_mod, graph64):
         assert np.array_equal(ids[i, :ks[i]], a.cpu().numpy().view(np.uint32)[0])
         assert np.array_equal(d[i, :ks[i]], b.cpu().numpy()[0])
         assert (ids[i, ks[i]:] == 0xFFFFFFFF).all()
+
+
+@pytest.mark.parametrize("store", ["f32", "u8"])
+def test_large_batch_in_any_order(oracle, vann_mod, graph64, store):
+    """A batch larger than the resident warps is taken farthest-from-the-entry first
+    (an order computed on the device); every query's result is still exactly the
+    oracle's, and a shuffled copy of the batch gives the same rows shuffled."""
+    import torch
+
+    base, g, entry = graph64
+    q = workload.mixture(6000, 128, 40, seed=91)
+    idx = _gpu_index(vann_mod, base, g, entry, stores=("f32", "u8"))
+    qd = torch.from_numpy(q).cuda()
+    ids, d = idx.search(qd, k=10, L=48, store=store)
+    st, oids, od, _, _ = g.search(q, 48, 10, entry, bloom_mode=oracle.BLOOM_SNAPSHOT)
+    assert st == 0
+    assert np.array_equal(ids.cpu().numpy().view(np.uint32), oids)
+    assert np.array_equal(d.cpu().numpy(), od)
+    perm = torch.from_numpy(np.random.default_rng(3).permutation(6000)).cuda()
+    ids2, d2 = idx.search(qd[perm].contiguous(), k=10, L=48, store=store)
+    assert torch.equal(ids2, ids[perm]) and torch.equal(d2, d[perm])
