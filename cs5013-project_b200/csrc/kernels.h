@@ -46,7 +46,6 @@ struct SearchArgs {
 
 cudaError_t launch_search(const SearchArgs& a, int store, int num_sms, cudaStream_t st, int variant = 0);
 int         search_variants();
-size_t      search_smem_per_warp(uint32_t L, uint32_t R, bool rerank);
 
 // RobustPrune over candidates A (expansion list or reverse entries) merged with
 // B (the node's current out-neighbours).

@@ -21,9 +21,4 @@ cudaError_t launch_search(const SearchArgs& a, int store, int num_sms, cudaStrea
 
 int search_variants() { return kSearchVariants; }
 
-size_t search_smem_per_warp(uint32_t L, uint32_t R, bool rerank) {
-    uint32_t maxr = R <= 32 ? 32 : (R <= 64 ? 64 : 128);
-    return SmemLayout::make(L, maxr, rerank).bytes;
-}
-
 }  // namespace vann
