@@ -442,6 +442,8 @@ def main():
                                    f"build R={R} L={L_BUILD} alpha={ALPHA} batches of {BATCH}; k={K}",
                        "headline_form": head, "L": hr["L"], "recall@10": round(hr["recall"], 4),
                        "l2": "flushed before every step (256 MB write)", "parallelism": f"replicas x{world}",
+                       "schedule": "queries taken farthest from the entry point first (order computed on the "
+                                   "device inside each timed step)",
                        "build_s": round(build_s, 2)},
             "p50_ms": round(p50, 4), "p99_ms": round(p99, 4),
             "forms": {nm: {"L": v["L"], "recall@10": round(v["recall"], 4), "qps": round(qps(nm), 1),
