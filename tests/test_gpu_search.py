@@ -196,3 +196,16 @@ def test_large_batch_in_any_order(oracle, vann_mod, graph64, store):
     perm = torch.from_numpy(np.random.default_rng(3).permutation(6000)).cuda()
     ids2, d2 = idx.search(qd[perm].contiguous(), k=10, L=48, store=store)
     assert torch.equal(ids2, ids[perm]) and torch.equal(d2, d[perm])
+
+
+def test_large_batch_of_equal_distances(vann_mod, graph64):
+    """A batch whose queries are all the same row puts every query in one order bucket
+    (zero distance range): each is still searched once, with the same result."""
+    import torch
+
+    base, g, entry = graph64
+    idx = _gpu_index(vann_mod, base, g, entry)
+    one = torch.from_numpy(base[17:18]).cuda()
+    ids, d = idx.search(one.repeat(5000, 1).contiguous(), k=10, L=32)
+    ref, rd = idx.search(one, k=10, L=32)
+    assert torch.equal(ids, ref.repeat(5000, 1)) and torch.equal(d, rd.repeat(5000, 1))
