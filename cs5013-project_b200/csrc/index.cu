@@ -221,6 +221,8 @@ struct vann_index {
     // per-query L / k arrays of the vann_search_uneven call in progress
     const uint32_t* pending_Lq = nullptr;
     const uint32_t* pending_kq = nullptr;
+    // launch-bound variant of the build and insert searches per row format (-1: not timed yet)
+    int build_variant[4] = {-1, -1, -1, -1};
     // autotuned search variant per (store, rerank, beam, L)
     std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>, int> tuned;
 
@@ -338,7 +340,7 @@ struct vann_index {
         const uint32_t* in_count   = nullptr;
         if (rev) {
             VCHECK(cudaMemsetAsync(rev_count, 0, sizeof(uint32_t), st));
-            VCHECK(vann::launch_prune_rev(pa, rev_list, rev_count, num_sms, st));
+            VCHECK(vann::launch_prune_rev(pa, u8_exact(st), rev_list, rev_count, num_sms, st));
             pa.counter = next_counter(st);
             in_list    = rev_list;
             in_count   = rev_count;
@@ -420,7 +422,33 @@ struct vann_index {
             a.store = store[3];
             sstore  = VANN_STORE_U8;
         }
-        VCHECK(vann::launch_search(a, sstore, num_sms, st));
+        // the first large batch of each row format times the launch-bound variants
+        // (the same search each time: the expansion lists do not depend on the variant)
+        if (build_variant[sstore] < 0 && count >= 4096) {
+            cudaEvent_t e0, e1;
+            VCHECK(cudaEventCreate(&e0));
+            VCHECK(cudaEventCreate(&e1));
+            float best_ms = 1e30f;
+            int   best    = 0;
+            for (int v = 0; v < vann::search_variants(); ++v) {
+                a.counter = next_counter(st);
+                VCHECK(cudaEventRecord(e0, st));
+                VCHECK(vann::launch_search(a, sstore, num_sms, st, v));
+                VCHECK(cudaEventRecord(e1, st));
+                VCHECK(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                VCHECK(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best    = v;
+                }
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            build_variant[sstore] = best;
+            a.counter = next_counter(st);
+        }
+        VCHECK(vann::launch_search(a, sstore, num_sms, st, std::max(build_variant[sstore], 0)));
 
         vann::PruneArgs pa{};
         pa.vecs = vecs;

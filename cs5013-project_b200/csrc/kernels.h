@@ -96,7 +96,8 @@ cudaError_t launch_prune_tc(const PruneArgs& a, const uint32_t* in_list, const u
                             cudaStream_t st);
 // Reverse re-prune of consistent lists, one warp per node (prune_rev.cu): nodes
 // with more than 128 candidates or 8 reverse sources are handed on in out_list.
-cudaError_t launch_prune_rev(const PruneArgs& a, uint32_t* out_list, uint32_t* out_count, int num_sms,
+// u8: distances from a.vecs_u8 (the host has read that every row is exact).
+cudaError_t launch_prune_rev(const PruneArgs& a, bool u8, uint32_t* out_list, uint32_t* out_count, int num_sms,
                              cudaStream_t st);
 
 // searchPoints2's merge of graph results with the insert list (staged.cu)

@@ -62,15 +62,18 @@ __device__ __forceinline__ void all_dists(const PruneArgs& a, const void* store,
         dists_to<S, DC>(a.vecs + (uint64_t)w.cid[i] * a.D, store, w.cid, nc, w.ad[i], a.D, lane);
 }
 
-template <int DC>
+// U8: distances from the exact uint8 rows (chosen on the host, which has read the
+// exactness flag); the kernel then holds one distance path only, which keeps its code
+// small enough for the instruction cache.  Should the flag say otherwise on the device,
+// every node is handed on to the next pass.
+template <int DC, bool U8>
 __global__ void __launch_bounds__(128) prune_rev_kernel(PruneArgs a, uint32_t* out_list, uint32_t* out_count) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t lane = threadIdx.x & 31u;
     RevWarp&       w    = reinterpret_cast<RevWarp*>(smem_raw)[threadIdx.x >> 5];
     const uint32_t R    = a.R;
-    // exact uint8 rows when the conversion found every row exact
-    const bool     u8   = a.vecs_u8 != nullptr && a.gate != nullptr &&
-                    *reinterpret_cast<volatile const uint32_t*>(a.gate) == 0u;
+    const bool     gated = U8 && (a.vecs_u8 == nullptr || a.gate == nullptr ||
+                                  *reinterpret_cast<volatile const uint32_t*>(a.gate) != 0u);
     uint32_t       done = 0;
 
     for (;;) {
@@ -85,7 +88,7 @@ __global__ void __launch_bounds__(128) prune_rev_kernel(PruneArgs a, uint32_t* o
         const uint32_t aoff = __ldg(a.csr_off + ci);
         const uint32_t nB   = a.use_b ? min(a.deg[node], R) : 0u;
         const uint32_t nc   = nA + nB;
-        if (nc > kMaxC || nA > kMaxA) {
+        if (nc > kMaxC || nA > kMaxA || gated) {
             if (lane == 0) out_list[atomicAdd(out_count, 1u)] = s;
             continue;
         }
@@ -94,12 +97,8 @@ __global__ void __launch_bounds__(128) prune_rev_kernel(PruneArgs a, uint32_t* o
         __syncwarp();
 
         // --- 1. distances
-        if (u8) {
-            if (a.D <= 128) all_dists<StoreU8, 0>(a, a.vecs_u8, w, node, nA, nc, lane);
-            else all_dists<StoreU8, 1>(a, a.vecs_u8, w, node, nA, nc, lane);
-        } else {
-            all_dists<StoreF32, DC>(a, a.vecs, w, node, nA, nc, lane);
-        }
+        if constexpr (U8) all_dists<StoreU8, DC>(a, a.vecs_u8, w, node, nA, nc, lane);
+        else all_dists<StoreF32, DC>(a, a.vecs, w, node, nA, nc, lane);
         __syncwarp();
 
         // --- 2. stable order by (distance, candidate index)
@@ -214,13 +213,14 @@ __global__ void __launch_bounds__(128) prune_rev_kernel(PruneArgs a, uint32_t* o
 
 }  // namespace
 
-cudaError_t launch_prune_rev(const PruneArgs& a, uint32_t* out_list, uint32_t* out_count, int num_sms,
+cudaError_t launch_prune_rev(const PruneArgs& a, bool u8, uint32_t* out_list, uint32_t* out_count, int num_sms,
                              cudaStream_t st) {
     if (a.n_nodes == 0) return cudaSuccess;
     if (!a.node_ids || !a.csr_off || !a.consistent || a.D > 256) return cudaErrorInvalidValue;
     const int    warps = 4;
     const size_t smem  = sizeof(RevWarp) * warps;
-    auto         kern  = a.D <= 128 ? prune_rev_kernel<0> : prune_rev_kernel<1>;
+    auto         kern  = a.D <= 128 ? (u8 ? prune_rev_kernel<0, true> : prune_rev_kernel<0, false>)
+                                    : (u8 ? prune_rev_kernel<1, true> : prune_rev_kernel<1, false>);
     cudaError_t  e     = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
