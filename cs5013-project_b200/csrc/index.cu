@@ -232,7 +232,9 @@ struct vann_index {
         return it == tuned.end() ? 0 : it->second;
     }
 
-    DevBuf ord;  // search order of large batches: distance keys, then the order
+    // search order of large batches (distance keys, then the order), one workspace per
+    // stream: searches in flight on different streams (the server's slots) never share it
+    std::map<cudaStream_t, DevBuf> ord;
     DevBuf vis_ids, vis_d, vis_n, nodes, runs, ovf, stage, s2_ids, s2_d, e_keys, e_vals, e_keys2, e_vals2, counts, offsets, cub_tmp,
         medoid_ws, gather, cand, cand_n, list_n, out_tmp;
 
@@ -250,7 +252,7 @@ struct vann_index {
         cudaFree(tomb);
         cudaFree(counters);
         cudaFree(status);
-        ord.release();
+        for (auto& o : ord) o.second.release();
         for (DevBuf* b : {&vis_ids, &vis_d, &vis_n, &nodes, &runs, &ovf, &stage, &s2_ids, &s2_d, &e_keys, &e_vals, &e_keys2, &e_vals2,
                           &counts, &offsets, &cub_tmp, &medoid_ws, &gather, &cand, &cand_n,
                           &list_n, &out_tmp})
@@ -272,8 +274,9 @@ struct vann_index {
     // warp runs a query when, never its result.
     const uint32_t* search_order(const float* d_queries, uint64_t nq, cudaStream_t st) {
         if (nq <= 16ull * (uint64_t)num_sms || nq > 0x7FFFFFFFull) return nullptr;
-        ord.ensure(sizeof(uint32_t) * 2 * nq);
-        uint32_t* keys  = ord.as<uint32_t>();
+        DevBuf& ob = ord[st];
+        ob.ensure(sizeof(uint32_t) * 2 * nq);
+        uint32_t* keys  = ob.as<uint32_t>();
         uint32_t* order = keys + nq;
         entry_dist_kernel<<<(unsigned)((nq + 7) / 8), 256, 0, st>>>(d_queries, nq, p.dim,
                                                                   vecs + (uint64_t)entry * p.dim, keys);

@@ -151,3 +151,25 @@ def test_group_commit_replays_by_epoch(vann_mod):
             alone.delete(torch.from_numpy(op[1].astype(np.int32)).cuda())
         else:
             alone.consolidate()
+
+
+def test_large_batches_in_flight_together(vann_mod):
+    """Batches larger than 16 queries per SM are ordered on the device before their
+    search; several such batches on the server's slot streams at once each keep their
+    own order workspace, so every result still equals the request run alone."""
+    import torch
+
+    base = workload.mixture(8000, 128, 30, seed=82)
+    idx = _index(vann_mod, base)
+    reqs = [workload.mixture(3000, 128, 30, seed=30_000 + i) for i in range(8)]
+    want = [idx.search(torch.from_numpy(r).cuda(), k=10, L=48) for r in reqs]
+    torch.cuda.synchronize()
+    srv = vann_mod.Server(idx, max_batch=6000, slots=4, max_k=10)
+    tickets = [srv.submit_search(r, 10, 48) for r in reqs]
+    for t, (wi, wd) in zip(tickets, want):
+        ids, d, _ = srv.wait(t)
+        assert np.array_equal(ids, wi.cpu().numpy().view(np.uint32))
+        assert np.array_equal(d, wd.cpu().numpy())
+    st = srv.stats()
+    assert st["max_inflight"] >= 2, st  # batches overlapped on the device
+    srv.close()
