@@ -455,7 +455,10 @@ def main():
                     "d2h_bytes_per_step": nq * K * 8,
                     "how": "C ABI search on pinned host queries; per step H2D + L2 flush (256 MB write) + "
                            "search + D2H, double-buffered on upload, compute and download streams"},
-            "gpu_launches": steps,
+            # per step: the search, and for a batch over 16 queries per SM the two kernels
+            # that order it (entry distances, bucket order)
+            "gpu_launches": steps * (3 if nq > 16 * torch.cuda.get_device_properties(dev).multi_processor_count
+                                     else 1),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "algorithmic_bytes_per_launch": bytes_head, "hops_per_query": round(hops_head, 2),
