@@ -77,6 +77,7 @@ class ServerStats(C.Structure):
 
 
 _lib = None
+ABI_VERSION = 2  # VANN_ABI_VERSION of include/vann.h that these ctypes structs mirror
 
 
 def lib():
@@ -131,6 +132,8 @@ def lib():
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
+        if L.vann_abi_version() != ABI_VERSION:  # the structs below must match the library's
+            raise ImportError(f"{LIB_PATH} has C ABI {L.vann_abi_version()}, this module needs {ABI_VERSION}")
         _lib = L
     return _lib
 

@@ -20,7 +20,8 @@
 extern "C" {
 #endif
 
-#define VANN_ABI_VERSION 1
+/* 2: vann_search_params gained `beam` (a caller built against 1 passes a shorter struct) */
+#define VANN_ABI_VERSION 2
 
 typedef enum {
     VANN_OK              = 0,

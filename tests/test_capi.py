@@ -26,7 +26,7 @@ def test_status_strings_and_abi_version():
     import vann
 
     L = vann.lib()
-    assert L.vann_abi_version() == 1
+    assert L.vann_abi_version() == vann.ABI_VERSION == 2
     assert L.vann_status_string(0) == b"ok"
     assert L.vann_status_string(5) == b"hop limit reached"
 

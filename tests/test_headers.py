@@ -16,7 +16,7 @@ def _compile(src: str, compiler: str, ext: str):
 
 
 def test_c_header_is_plain_c():
-    _compile('#include "vann.h"\nint main(void){ vann_params p; (void)p; return vann_abi_version() == 1 ? 0 : 1; }\n',
+    _compile('#include "vann.h"\nint main(void){ vann_params p; (void)p; return vann_abi_version() == VANN_ABI_VERSION ? 0 : 1; }\n',
              "gcc", ".c")
 
 
