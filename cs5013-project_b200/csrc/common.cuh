@@ -93,7 +93,8 @@ struct StoreBF16 {
 struct StoreFP8 {
     static constexpr int  kElems = 16, kLanes128 = 8, kM = 8;
     static constexpr bool kScaled = true, kInt = false;
-    __device__ __forceinline__ static void widen(const uint4& r, float s, float (&o)[16]) {
+    // the 16 codes of a chunk as floats, unscaled (e4m3 -> f16 -> f32 is exact)
+    __device__ __forceinline__ static void codes(const uint4& r, float (&o)[16]) {
         const uint32_t w[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
@@ -101,11 +102,16 @@ struct StoreFP8 {
             __half2_raw hi = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[i] >> 16), __NV_E4M3);
             float2 a = __half22float2(*reinterpret_cast<__half2*>(&lo));
             float2 b = __half22float2(*reinterpret_cast<__half2*>(&hi));
-            o[4 * i]     = a.x * s;
-            o[4 * i + 1] = a.y * s;
-            o[4 * i + 2] = b.x * s;
-            o[4 * i + 3] = b.y * s;
+            o[4 * i]     = a.x;
+            o[4 * i + 1] = a.y;
+            o[4 * i + 2] = b.x;
+            o[4 * i + 3] = b.y;
         }
+    }
+    __device__ __forceinline__ static void widen(const uint4& r, float s, float (&o)[16]) {
+        codes(r, o);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) o[i] *= s;
     }
 };
 struct StoreU8 {
@@ -153,6 +159,7 @@ struct Query {
     uint32_t     u[Layout<S, DC>::kCPL][S::kElems / 4];
     const float* row;
     int          qq;
+    float        qn;  // this lane's share of |q|^2 (scaled stores)
     bool         qint;
 };
 
@@ -163,6 +170,7 @@ __device__ __forceinline__ void load_query(Query<S, DC>& q, const float* row, ui
     const uint32_t t      = lane % Ly::kT;
     bool           ok     = true;
     int            qq     = 0;
+    float          qn     = 0.f;
 #pragma unroll
     for (int c = 0; c < Ly::kCPL; ++c) {
         uint32_t k     = t + (uint32_t)Ly::kT * c;
@@ -176,6 +184,7 @@ __device__ __forceinline__ void load_query(Query<S, DC>& q, const float* row, ui
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 if constexpr (!S::kInt) q.f[c][4 * v + i] = e[i];
+                if constexpr (S::kScaled) qn = fmaf(e[i], e[i], qn);
                 bool good = e[i] >= 0.f && e[i] <= 255.f && rintf(e[i]) == e[i];
                 ok &= good;
                 uint32_t b = good ? (uint32_t)e[i] : 0u;
@@ -186,6 +195,7 @@ __device__ __forceinline__ void load_query(Query<S, DC>& q, const float* row, ui
         }
     }
     q.row  = row;
+    q.qn   = qn;
     q.qint = __all_sync(0xffffffffu, ok);
     // each group of T lanes holds the whole query
 #pragma unroll
@@ -295,6 +305,28 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
             int y = group_reduce<M, Ly::kT, int>(v, lane);
             return (float)(y + q.qq);
         }
+    }
+    if constexpr (S::kScaled) {
+        // sum (q - s c)^2 = |q|^2 - 2 s (q . c) + s^2 |c|^2: the codes are widened
+        // unscaled, and each row's scale is applied once, not once per element
+        float v[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            float qc = 0.f, cc = 0.f;
+#pragma unroll
+            for (int c = 0; c < Ly::kCPL; ++c) {
+                float e[S::kElems];
+                S::codes(x[m][c], e);
+#pragma unroll
+                for (int i = 0; i < S::kElems; ++i) {
+                    qc = fmaf(q.f[c][i], e[i], qc);
+                    cc = fmaf(e[i], e[i], cc);
+                }
+            }
+            v[m] = fmaf(sc[m] * sc[m], cc, fmaf(-2.f * sc[m], qc, q.qn));
+        }
+        // rounding can leave a tiny negative for a row equal to the query
+        return fmaxf(group_reduce<M, Ly::kT, float>(v, lane), 0.f);
     }
     float v[M];
 #pragma unroll
