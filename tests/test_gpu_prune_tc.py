@@ -34,6 +34,19 @@ def test_one_batch_build_matches_oracle(oracle, vann_mod, R, L):
     assert _rows_equal(deg, adj, og.deg, og.adj) == []
 
 
+@pytest.mark.parametrize("stores", [("f32", "u8"), ("f32",)])
+def test_large_batch_build_matches_oracle(oracle, vann_mod, stores):
+    """One batch of 6,000 rows: its search is ordered on the device and its first run
+    times the launch-bound variants; the graph is still the oracle's, row for row."""
+    base = workload.mixture(6000, 128, 40, seed=141)
+    og, entry = oracle.build_index(base, R=32, L=64, alpha=1.2, seed=7, skip_mode=2,
+                                   bloom_mode=oracle.BLOOM_SNAPSHOT)
+    idx = _build(vann_mod, base, 32, 64, stores)
+    assert idx.info()["entry"] == entry
+    _, deg, adj = idx.get_graph()
+    assert _rows_equal(deg, adj, og.deg, og.adj) == []
+
+
 def test_batched_build_and_insert_equal_cuda_core_path(vann_mod):
     import torch
 
