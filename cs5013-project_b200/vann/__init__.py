@@ -245,7 +245,7 @@ class Index:
         return ids, dists
 
     def search_uneven(self, queries, L, k, store: str = "f32", rerank: bool = False, quirks: int = 0,
-                      stream=None):
+                      stream=None, beam: int = 1):
         """One launch over queries with their own L[i] and k[i] (int32 CUDA tensors);
         returns (ids, dists) with max(k) columns, padded past k[i]."""
         torch = _torch()
@@ -253,7 +253,7 @@ class Index:
         Lmax, kmax = int(L.max().item()), int(k.max().item())
         ids = torch.empty((nq, kmax), dtype=torch.int32, device=queries.device)
         dists = torch.empty((nq, kmax), dtype=torch.float32, device=queries.device)
-        sp = SearchParams(Lmax, kmax, STORES[store], int(rerank), quirks, 0)
+        sp = SearchParams(Lmax, kmax, STORES[store], int(rerank), quirks, 0, beam)
         _check(lib().vann_search_uneven(self._h, _dev(queries, torch.float32), nq, C.byref(sp),
                                         _dev(L, torch.int32), _dev(k, torch.int32), _dev(ids, torch.int32),
                                         _dev(dists, torch.float32), _stream_ptr(stream)))

@@ -63,3 +63,23 @@ def test_beam2_recall_hops_and_limits(oracle, vann_mod):
     with pytest.raises(vann_mod.VannError) as e:
         idx.search(qd, k=10, L=32, beam=3)
     assert e.value.status == vann_mod.ERR_INVALID
+
+
+def test_beam2_uneven_batch_equals_separate_launches(vann_mod, graph):
+    """Per-query L and k with two parents per hop: each row is the separate search's."""
+    import torch
+
+    base, g, entry = graph
+    q = workload.mixture(64, 128, 20, seed=126)
+    idx = vann_mod.Index(128, 32, 64, 1.2, capacity=2000, stores=("f32", "u8"))
+    idx.set_graph(base, g.deg, g.adj, entry, consistent=True)
+    rng = np.random.default_rng(4)
+    ks = rng.choice([1, 5, 10], 64).astype(np.int32)
+    Ls = np.maximum(ks, rng.integers(8, 65, 64)).astype(np.int32)
+    qd = torch.from_numpy(q).cuda()
+    ids, d = idx.search_uneven(qd, torch.from_numpy(Ls).cuda(), torch.from_numpy(ks).cuda(), store="u8", beam=2)
+    ids, d = ids.cpu().numpy().view(np.uint32), d.cpu().numpy()
+    for i in range(64):
+        a, b = idx.search(qd[i:i + 1].contiguous(), k=int(ks[i]), L=int(Ls[i]), store="u8", beam=2)
+        assert np.array_equal(ids[i, :ks[i]], a.cpu().numpy().view(np.uint32)[0])
+        assert np.array_equal(d[i, :ks[i]], b.cpu().numpy()[0])
