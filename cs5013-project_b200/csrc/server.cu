@@ -151,10 +151,14 @@ struct vann_server {
         if (rows == 0) return false;
         s.kmax = kmax;
         vann_search_params sp{Lmax, kmax, p.store, p.rerank, 0, 0};
-        cudaMemcpyAsync(s.d_q, s.h_q, sizeof(float) * rows * dim, cudaMemcpyHostToDevice, s.st);
-        cudaMemcpyAsync(s.d_L, s.h_L, sizeof(uint32_t) * rows, cudaMemcpyHostToDevice, s.st);
-        cudaMemcpyAsync(s.d_k, s.h_k, sizeof(uint32_t) * rows, cudaMemcpyHostToDevice, s.st);
-        vann_status st = vann_search_uneven(idx, s.d_q, rows, &sp, s.d_L, s.d_k, s.d_ids, s.d_d, s.st);
+        cudaError_t ce = cudaMemcpyAsync(s.d_q, s.h_q, sizeof(float) * rows * dim, cudaMemcpyHostToDevice, s.st);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(s.d_L, s.h_L, sizeof(uint32_t) * rows, cudaMemcpyHostToDevice, s.st);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(s.d_k, s.h_k, sizeof(uint32_t) * rows, cudaMemcpyHostToDevice, s.st);
+        vann_status st = ce == cudaSuccess
+                             ? vann_search_uneven(idx, s.d_q, rows, &sp, s.d_L, s.d_k, s.d_ids, s.d_d, s.st)
+                             : VANN_ERR_CUDA;
         if (st != VANN_OK) {
             for (auto& rr : s.reqs) complete(rr.first, st);
             s.reqs.clear();
@@ -162,9 +166,17 @@ struct vann_server {
             cv_done.notify_all();
             return false;
         }
-        cudaMemcpyAsync(s.h_ids, s.d_ids, sizeof(uint32_t) * rows * kmax, cudaMemcpyDeviceToHost, s.st);
-        cudaMemcpyAsync(s.h_d, s.d_d, sizeof(float) * rows * kmax, cudaMemcpyDeviceToHost, s.st);
-        cudaEventRecord(s.done, s.st);
+        ce = cudaMemcpyAsync(s.h_ids, s.d_ids, sizeof(uint32_t) * rows * kmax, cudaMemcpyDeviceToHost, s.st);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(s.h_d, s.d_d, sizeof(float) * rows * kmax, cudaMemcpyDeviceToHost, s.st);
+        if (ce == cudaSuccess) ce = cudaEventRecord(s.done, s.st);
+        if (ce != cudaSuccess) {  // the results would never arrive: fail the batch now
+            for (auto& rr : s.reqs) complete(rr.first, VANN_ERR_CUDA);
+            s.reqs.clear();
+            last_error = cudaGetErrorString(ce);
+            cv_done.notify_all();
+            return false;
+        }
         s.busy = true;
         ++n_batches;
         n_searched += rows;
@@ -190,19 +202,25 @@ struct vann_server {
             if (stage_sz == 0) return VANN_ERR_OOM;
             float*    dv = static_cast<float*>(d_stage);
             uint32_t* di = reinterpret_cast<uint32_t*>(dv + (size_t)r->n * dim);
-            cudaMemcpyAsync(dv, r->vecs.data(), sizeof(float) * r->n * dim, cudaMemcpyHostToDevice, wst);
+            if (cudaMemcpyAsync(dv, r->vecs.data(), sizeof(float) * r->n * dim, cudaMemcpyHostToDevice, wst) !=
+                cudaSuccess)
+                return VANN_ERR_CUDA;
             st = vann_insert(idx, dv, r->n, di, wst);
             if (st == VANN_OK) {
                 r->out_ids.resize(r->n);
-                cudaMemcpyAsync(r->out_ids.data(), di, sizeof(uint32_t) * r->n, cudaMemcpyDeviceToHost, wst);
-                cudaStreamSynchronize(wst);
+                if (cudaMemcpyAsync(r->out_ids.data(), di, sizeof(uint32_t) * r->n, cudaMemcpyDeviceToHost, wst) !=
+                        cudaSuccess ||
+                    cudaStreamSynchronize(wst) != cudaSuccess)
+                    st = VANN_ERR_CUDA;
             }
         } else if (r->kind == kDelete) {
             stage(sizeof(uint32_t) * r->n);
             if (stage_sz == 0) return VANN_ERR_OOM;
-            cudaMemcpyAsync(d_stage, r->ids.data(), sizeof(uint32_t) * r->n, cudaMemcpyHostToDevice, wst);
+            if (cudaMemcpyAsync(d_stage, r->ids.data(), sizeof(uint32_t) * r->n, cudaMemcpyHostToDevice, wst) !=
+                cudaSuccess)
+                return VANN_ERR_CUDA;
             st = vann_delete(idx, static_cast<uint32_t*>(d_stage), r->n, wst);
-            cudaStreamSynchronize(wst);
+            if (st == VANN_OK && cudaStreamSynchronize(wst) != cudaSuccess) st = VANN_ERR_CUDA;
         } else {
             st = vann_consolidate(idx, wst);
         }
