@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=10000)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the float-row precision sub-run and the request-latency burst")
     ap.add_argument("--profile", action="store_true", help="short run for a profiler capture")
     ap.add_argument("--only", default=None,
                     help="FORM@L (e.g. u8@32): sweep and time that one form at that L only, no autotune "
@@ -333,21 +335,23 @@ def main():
     p50 = float(np.percentile(hr["ms"], 50))
     p99 = float(np.percentile(hr["ms"], 99))
 
-    # work counters of the headline and FP32 forms (algorithmic bytes)
-    def counted_bytes(name):
+    # work per query of a form: hops, distance evaluations and adjacency words, as the
+    # kernel counts them (the oracle's counts replace these below where they apply)
+    def kernel_counts(name):
         _, store, rr, beam = form_of[name]
         _, _, st = idx.search_stats(q_d, k=K, L=results[name]["L"], store=store, rerank=rr, beam=beam)
         st = st.cpu().numpy().astype(np.int64)
-        hops, evals, adjw = st[0], st[1], st[2]
+        return st[0], st[1], st[2]
+
+    def algorithmic_bytes(name, hops, evals, adjw):
+        _, store, rr, _ = form_of[name]
         s = {"f32": 4, "bf16": 2, "u8": 1, "fp8": 1}[store]
         sc = 4 if store == "fp8" else 0
         L = results[name]["L"]
         per_q = (hops * 4 + adjw * 4 + evals * (DIM * s + sc) + 4 * DIM + 8 * K
                  + (min(L, 1 << 30) * 4 * DIM if rr else 0))
-        return float(per_q.sum()), float(hops.mean()), float(evals.mean())
+        return float(per_q.sum())
 
-    bytes_head, hops_head, evals_head = counted_bytes(head)
-    hops_f32 = counted_bytes("f32")[1] if "f32" in results else None
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -357,7 +361,6 @@ def main():
     peak = peaks.get("hbm_gbs", 6650.0)
     peak_source = ("MEASURED_PEAKS.json hbm_gbs (burst), of measured" if "hbm_gbs" in peaks
                    else "fallback 6650 GB/s (no MEASURED_PEAKS.json), of fallback")
-    achieved = bytes_head / (mean_ms / 1e3) / 1e9
     # DRAM bytes per launch of this kernel and workload, from the committed ncu capture
     traffic = None
     try:
@@ -427,10 +430,32 @@ def main():
     value   = replica_throughput(world, nq * steps, total_s)
     e2e_qps = replica_throughput(world, nq * steps, e2e_total)
 
-    # ---- CPU baseline: the oracle's search (same semantics as the FP32 form)
-    cpu = None
+    # ---- the oracle leg (rank 0 of a single-GPU run): FP32 id parity on this graph,
+    # the work counts of the roofline, and the CPU baseline
+    cpu, parity, work_by = None, None, "kernel counters (vann_search_stats)"
+    hh, he, ha = kernel_counts(head)
     if rank == 0 and world == 1 and not args.no_cpu and "f32" in results:
-        cpu = cpu_baseline(idx, q, results["f32"]["L"], args.cpu_sample, hops_f32, args.cpu_seconds)
+        leg = oracle_leg(torch, idx, q, q_d, results["f32"]["L"], args.cpu_sample, args.cpu_seconds)
+        cpu, parity = leg["cpu"], leg["parity"]
+        _, hstore, hrr2, hbeam2 = form_of[head]
+        # integer rows are exact in the uint8 and BF16 copies: those forms (one parent
+        # per hop, no rerank) take the FP32 form's trajectories, which the oracle counts
+        if hstore in ("u8", "bf16", "f32") and not hrr2 and hbeam2 == 1:
+            oc = leg["counts"] if results[head]["L"] == results["f32"]["L"] else \
+                oracle_counts(idx, q, results[head]["L"], args.cpu_sample)
+            if len(oc[0]) == nq:
+                hh, he, ha = oc
+                work_by = (f"the oracle's GreedySearch over the same graph and queries at L={results[head]['L']} "
+                           f"(integer rows: the {head} form's trajectories are the FP32 form's)")
+    bytes_head = algorithmic_bytes(head, hh, he, ha)
+    hops_head, evals_head = float(np.mean(hh)), float(np.mean(he))
+    achieved = bytes_head / (mean_ms / 1e3) / 1e9
+
+    # ---- the reduced-precision forms on float rows and per-request latency (single GPU)
+    precision, latency = None, None
+    if rank == 0 and world == 1 and not args.only and not args.profile and not args.no_extras:
+        precision = precision_subrun(torch, vann, dev, min(steps, 20), warm)
+        latency = latency_burst(torch, vann, idx, q, hr["L"], hs)
 
     if rank == 0:
         line = {
@@ -446,9 +471,12 @@ def main():
                        "schedule": "queries taken farthest from the entry point first (order computed on the "
                                    "device inside each timed step)",
                        "build_s": round(build_s, 2)},
-            "p50_ms": round(p50, 4), "p99_ms": round(p99, 4),
+            # percentiles of whole 10k-query steps (batches); per-request latency is in
+            # "request_latency"
+            "batch_p50_ms": round(p50, 4), "batch_p99_ms": round(p99, 4),
             "forms": {nm: {"L": v["L"], "recall@10": round(v["recall"], 4), "qps": round(qps(nm), 1),
-                           "p99_ms": round(float(np.percentile(v["ms"], 99)), 4)} for nm, v in results.items()},
+                           "batch_p99_ms": round(float(np.percentile(v["ms"], 99)), 4)}
+                      for nm, v in results.items()},
             "speedup_vs_fp32_plain": round(qps(head) / qps("f32"), 3) if "f32" in results else None,
             "autotune_ms_per_variant": tune_ms,
             "sweep": {nm: [[L, round(r, 4)] for L, r in v] for nm, v in sweep.items()},
@@ -463,22 +491,41 @@ def main():
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "algorithmic_bytes_per_launch": bytes_head, "hops_per_query": round(hops_head, 2),
-                         "evals_per_query": round(evals_head, 1), "peak_source": peak_source},
+                         "evals_per_query": round(evals_head, 1), "work_counted_by": work_by,
+                         "peak_source": peak_source,
+                         "limiter": "instruction issue and the dependent list -> rows load chain of each hop, "
+                                    "not DRAM bandwidth (ncu: profiles/search_u8_1Mx128.md)"},
             "clocks": clocks,
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if parity:
+            line["parity"] = parity
+        if precision:
+            line["precision"] = precision
+        if latency:
+            line["request_latency"] = latency
         if world == 1 and not args.only and not args.profile:
             # beside the reference arm's "reference_gpu": the same graph, queries and L
             line["at_reference_gpu_config"] = at_ref_config(torch, vann, dev)
         print(json.dumps(line), flush=True)
+        if parity and not parity["all_equal"]:
+            print("FP32 search differs from the oracle on the benchmark graph", file=sys.stderr)
+            if dist is not None:
+                dist.destroy_process_group()
+            return 3
     if dist is not None:
         dist.destroy_process_group()
     return 0
 
 
-def cpu_baseline(idx, q, L, sample, hops_f32, seconds):
-    """Times the oracle port of the reference search over a bounded query sample."""
+def oracle_leg(torch, idx, q, q_d, L, sample, seconds):
+    """The oracle's GreedySearch (oracle/vann_oracle.c, the reference's search.cuh restated)
+    over this index's graph: (1) parity -- the first `sample` queries at the FP32 form's
+    L against the GPU FP32 form, per query ids, distances, hop, distance-evaluation and
+    adjacency-word counts, all required equal; (2) the oracle's work counts of that
+    search; (3) the CPU baseline -- the same search repeated on all host threads for at
+    least `seconds`."""
     from oracle import oracle as O
 
     O.build()
@@ -487,17 +534,139 @@ def cpu_baseline(idx, q, L, sample, hops_f32, seconds):
     entry = idx.info()["entry"]
     threads = os.cpu_count() or 1
     qs = q[:sample]
-    done, dt, reps = 0, 0.0, 0
+    ids, d, st = idx.search_stats(q_d[:len(qs)].contiguous(), k=K, L=L, store="f32")
+    idx.sync()
+    gi, gd, gs = ids.cpu().numpy().view(np.uint32), d.cpu().numpy(), st.cpu().numpy().astype(np.int64)
+    done, dt, reps, first = 0, 0.0, 0, None
     while dt < seconds or reps == 0:
         t0 = time.time()
-        st, ids, d, hops, evals = g.search(qs, L, K, entry, threads=threads)
+        r = g.search(qs, L, K, entry, bloom_mode=O.BLOOM_SNAPSHOT, threads=threads, with_adjw=True)
         dt += time.time() - t0
         done += len(qs)
         reps += 1
-    return {"value": round(done / dt, 1), "unit": "queries/s", "cores": threads, "kind": "port",
-            "sample": f"{len(qs)} queries x {reps} passes ({dt:.1f} s) at L={L} (FP32), "
-                      f"oracle/vann_oracle.c GreedySearch, {threads} threads; mean hops {hops.mean():.2f} "
-                      f"(GPU kernel counted {hops_f32:.2f})"}
+        first = first or r
+    ost, oids, od, oh, oe, oa = first
+    eq = {"ids_equal": int((gi == oids).all(1).sum()), "dists_equal": int((gd == od).all(1).sum()),
+          "hops_equal": int((gs[0] == oh).sum()), "evals_equal": int((gs[1] == oe).sum()),
+          "adj_words_equal": int((gs[2] == oa).sum())}
+    parity = {"queries": len(qs), "form": "f32", "L": L, "k": K, **eq,
+              "all_equal": ost == 0 and all(v == len(qs) for v in eq.values()),
+              "oracle": "oracle/vann_oracle.c GreedySearch (vamana/include/search.cuh:20-367 restated), "
+                        "same graph, queries, entry and L"}
+    cpu = {"value": round(done / dt, 1), "unit": "queries/s", "cores": threads, "kind": "port",
+           "sample": f"{len(qs)} queries x {reps} passes ({dt:.1f} s) at L={L} (FP32), "
+                     f"oracle/vann_oracle.c GreedySearch, {threads} threads; mean hops {oh.mean():.2f}"}
+    return {"cpu": cpu, "parity": parity, "counts": (oh.astype(np.int64), oe, oa)}
+
+
+def oracle_counts(idx, q, L, sample):
+    """Hops, distance evaluations and adjacency words per query of the oracle's search at L."""
+    from oracle import oracle as O
+
+    vecs, deg, adj = idx.get_graph()
+    g = O.Graph(vecs, deg, adj)
+    _, _, _, oh, oe, oa = g.search(q[:sample], L, K, idx.info()["entry"], bloom_mode=O.BLOOM_SNAPSHOT,
+                                   threads=os.cpu_count() or 1, with_adjw=True)
+    return oh.astype(np.int64), oe, oa
+
+
+def precision_subrun(torch, vann, dev, steps, warm, n=1_000_000, nq=10_000, D=96):
+    """The reduced-precision configuration's recipe at a size that fits the default run:
+    n x 96 float rows from 2,000 unit-norm centres, sigma 0.05 (the 5M x 96 workload of
+    `--config precision`, a fifth of its rows), nq queries.  FP32, BF16+rerank and
+    FP8-E4M3 (per-row scale)+rerank traversal at L in {64, 128}: recall@10, QPS, and the
+    traversal and returned distance errors against FP64."""
+    from vann import workload
+
+    base = workload.mixture(n, D, 2000, seed=11, sigma=0.05, integer=False, unit_norm=True)
+    q = workload.mixture(nq, D, 2000, seed=12, sigma=0.05, integer=False, unit_norm=True)
+    base_d = torch.from_numpy(base).to(dev)
+    q_d = torch.from_numpy(q).to(dev)
+    del base
+    idx = vann.Index(D, R, L_BUILD, ALPHA, capacity=n, stores=("f32", "bf16", "fp8"))
+    t0 = time.time()
+    idx.build(base_d, batch=BATCH, seed=2024)
+    torch.cuda.synchronize()
+    build_s = time.time() - t0
+    gt = ground_truth(torch, base_d, q_d, K)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def rel_err(ids, d):
+        x = base_d[ids.clamp(min=0).long()].double()
+        exact = ((x - q_d.double()[:, None, :]) ** 2).sum(-1)
+        return ((d.double() - exact).abs() / exact.clamp(min=1e-30))[ids >= 0]
+
+    res = {}
+    for L in (64, 128):
+        for store, rr in (("f32", False), ("bf16", True), ("fp8", True)):
+            name = f"{store}{'+rerank' if rr else ''}@L{L}"
+            idx.autotune(q_d, k=K, L=L, store=store, rerank=rr)
+            ids, d = idx.search(q_d, k=K, L=L, store=store, rerank=rr)
+            t = time_steps(torch, lambda s=store, rr=rr, L=L: idx.search(q_d, k=K, L=L, store=s, rerank=rr),
+                           steps, warm, flush)
+            ent = {"recall@10": round(recall(torch, ids, gt), 4), "qps": round(nq / (statistics.mean(t) / 1e3), 1),
+                   "returned_max_rel_err": float(rel_err(ids, d).max())}
+            if store != "f32":
+                ids2, d2 = idx.search(q_d, k=K, L=L, store=store, rerank=False)
+                e2 = rel_err(ids2, d2)
+                ent["traversal_max_rel_err"] = float(e2.max())
+                ent["traversal_mean_rel_err"] = float(e2.mean())
+                ent["recall@10_no_rerank"] = round(recall(torch, ids2, gt), 4)
+            res[name] = ent
+    for L in (64, 128):
+        f = res[f"f32@L{L}"]
+        for s in ("bf16+rerank", "fp8+rerank"):
+            e = res[f"{s}@L{L}"]
+            e["recall_loss_vs_f32"] = round(f["recall@10"] - e["recall@10"], 4)
+            e["speedup_vs_f32"] = round(e["qps"] / f["qps"], 3)
+    del idx, base_d, q_d, flush
+    torch.cuda.empty_cache()
+    return {"workload": f"{n}x{D} float32, 2000 unit-norm centres, sigma 0.05 (the 5Mx96 recipe at {n} rows); "
+                        f"{nq} queries; R={R} L={L_BUILD} alpha={ALPHA}; k={K}; L2 flushed before every step",
+            "build_s": round(build_s, 2), "forms": res}
+
+
+def latency_burst(torch, vann, idx, q, L, store, rate=50_000.0, duration=1.0):
+    """Per-request latency: a Poisson stream of single-query searches (k=10 at the headline
+    form's L and row format) offered at `rate` for `duration` seconds to the continuous-
+    batching server over the benchmark index.  Latency is measured by the server from
+    submission to completion of each request (host queries in, host results out)."""
+    import threading as th
+
+    srv = vann.Server(idx, max_batch=4096, slots=4, max_k=K, store=store)
+    rng = np.random.default_rng(17)
+    nreq = int(rate * duration)
+    gaps = rng.exponential(1.0 / rate, nreq)
+    pick = rng.integers(0, len(q), nreq)
+    tickets, results = [None] * nreq, [None] * nreq
+
+    def waiter():
+        for i in range(nreq):
+            while tickets[i] is None:
+                time.sleep(0.0002)
+            results[i] = srv.wait(tickets[i])
+
+    w = th.Thread(target=waiter)
+    w.start()
+    t_start = time.perf_counter()
+    t_next = t_start
+    for i in range(nreq):
+        t_next += gaps[i]
+        while time.perf_counter() < t_next:
+            pass
+        tickets[i] = srv.submit_search(q[pick[i]], K, L)
+    w.join()
+    t_end = time.perf_counter()
+    stats = srv.stats()
+    srv.close()
+    lat_ms = np.array([r[2] for r in results]) / 1e3
+    return {"how": f"Poisson stream of single-query searches (k={K}, L={L}, {store} rows) offered at "
+                   f"{rate:.0f} req/s for {duration} s to vann_server (4 slots, batches up to 4096) over "
+                   f"the benchmark index; per-request time from submit to completion",
+            "requests": nreq, "achieved_req_per_s": round(nreq / (t_end - t_start), 1),
+            "p50_ms": round(float(np.percentile(lat_ms, 50)), 3),
+            "p99_ms": round(float(np.percentile(lat_ms, 99)), 3),
+            "max_ms": round(float(lat_ms.max()), 3), "batches": stats["batches"]}
 
 
 def main_reference():

@@ -5,6 +5,7 @@
 #include <cuda_fp8.h>
 
 #include <mutex>
+#include <string>
 
 #include "../../include/vann.h"
 #include "common.cuh"
@@ -164,24 +165,54 @@ cudaError_t launch_set_bits(uint32_t* bits, const uint32_t* ids, uint64_t n, uin
 }
 
 // Medoid = argmin_i ||x_i - mean||^2 in FP64, smallest id on ties
-// (parth/tools/vamana.py:25-29).  mean_ws: D doubles; best_ws: [min bits, id].
-__global__ void col_sum_kernel(const float* vecs, uint64_t n, uint32_t D, double* sum) {
-    uint32_t d  = threadIdx.x + blockIdx.y * blockDim.x;
-    if (d >= D) return;
-    uint64_t r0 = blockIdx.x * (uint64_t)1024;
-    uint64_t r1 = n < r0 + 1024 ? n : r0 + 1024;
-    double   s  = 0.0;
-    for (uint64_t r = r0; r < r1; ++r) s += (double)vecs[r * D + d];
-    atomicAdd(sum + d, s);
+// (parth/tools/vamana.py:25-29).  The column sums do not depend on the order in
+// which blocks add them, so the medoid is the same on every run: each element is
+// put on a fixed-point grid of its column, x * 2^(B - e_d), where 2^e_d bounds the
+// column's magnitudes and n * 2^B < 2^63, and the terms are added as 64-bit
+// integers, which is exact.  For integer-valued rows every term is exact and the
+// means equal a sequential FP64 sum divided by n.  The squared distances to the
+// mean are summed sequentially over d without contraction (as the oracle does).
+__device__ __forceinline__ int column_exponent(uint32_t bound_bits) {
+    if (bound_bits == 0u) return 0;
+    int e = 0;
+    frexpf(__uint_as_float(bound_bits), &e);  // bound < 2^e
+    return e;
 }
-__global__ void medoid_dist_kernel(const float* vecs, uint64_t n, uint32_t D, const double* sum,
+__global__ void col_bound_kernel(const float* vecs, uint64_t n, uint32_t D, uint32_t* bound) {
+    const uint32_t d = threadIdx.x + blockIdx.y * blockDim.x;
+    if (d >= D) return;
+    const uint64_t r0 = blockIdx.x * (uint64_t)1024;
+    const uint64_t r1 = n < r0 + 1024 ? n : r0 + 1024;
+    uint32_t       m  = 0u;
+    for (uint64_t r = r0; r < r1; ++r) m = max(m, __float_as_uint(fabsf(vecs[r * D + d])));
+    atomicMax(bound + d, m);
+}
+__global__ void col_sum_kernel(const float* vecs, uint64_t n, uint32_t D, const uint32_t* bound, int B,
+                               unsigned long long* sum) {
+    const uint32_t d = threadIdx.x + blockIdx.y * blockDim.x;
+    if (d >= D) return;
+    const int      sh = B - column_exponent(bound[d]);
+    const uint64_t r0 = blockIdx.x * (uint64_t)1024;
+    const uint64_t r1 = n < r0 + 1024 ? n : r0 + 1024;
+    long long      s  = 0;
+    for (uint64_t r = r0; r < r1; ++r) s += llrint(ldexp((double)vecs[r * D + d], sh));
+    atomicAdd(sum + d, (unsigned long long)s);
+}
+// in place: the integer column sums become FP64 means
+__global__ void col_mean_kernel(uint64_t n, uint32_t D, const uint32_t* bound, int B, unsigned long long* sum) {
+    const uint32_t d = threadIdx.x + blockIdx.x * blockDim.x;
+    if (d >= D) return;
+    const long long s = (long long)sum[d];
+    reinterpret_cast<double*>(sum)[d] = ldexp((double)s, column_exponent(bound[d]) - B) / (double)n;
+}
+__global__ void medoid_dist_kernel(const float* vecs, uint64_t n, uint32_t D, const double* mean,
                                    unsigned long long* best, int pass) {
     uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (r >= n) return;
     double s = 0.0;
     for (uint32_t d = 0; d < D; ++d) {
-        double t = (double)vecs[r * D + d] - sum[d] / (double)n;
-        s += t * t;
+        const double t = (double)vecs[r * D + d] - mean[d];
+        s              = __dadd_rn(s, __dmul_rn(t, t));
     }
     unsigned long long bits = (unsigned long long)__double_as_longlong(s);
     if (pass == 0)
@@ -189,18 +220,42 @@ __global__ void medoid_dist_kernel(const float* vecs, uint64_t n, uint32_t D, co
     else if (bits == best[0])
         atomicMin(best + 1, (unsigned long long)r);
 }
-cudaError_t launch_medoid(const float* vecs, uint64_t n, uint32_t D, double* mean_ws,
-                          unsigned long long* best_ws, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(mean_ws, 0, sizeof(double) * D, st);
+__global__ void medoid_result_kernel(const unsigned long long* best, uint32_t* out) { *out = (uint32_t)best[1]; }
+
+static size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
+size_t medoid_ws_bytes(uint32_t D) { return align16(sizeof(double) * D) + align16(sizeof(uint32_t) * D) + 16; }
+unsigned long long* medoid_best(void* ws, uint32_t D) {
+    return reinterpret_cast<unsigned long long*>(static_cast<char*>(ws) + align16(sizeof(double) * D) +
+                                                 align16(sizeof(uint32_t) * D));
+}
+cudaError_t launch_medoid(const float* vecs, uint64_t n, uint32_t D, void* ws, uint32_t* d_out, cudaStream_t st) {
+    if (n == 0 || D == 0) return cudaErrorInvalidValue;
+    auto*               sum   = static_cast<unsigned long long*>(ws);
+    auto*               bound = reinterpret_cast<uint32_t*>(static_cast<char*>(ws) + align16(sizeof(double) * D));
+    unsigned long long* best  = medoid_best(ws, D);
+    int lg = 1;  // ceil(log2(n)), at least 1
+    while (lg < 63 && (1ull << lg) < n) ++lg;
+    const int   B = 62 - lg;
+    cudaError_t e = cudaMemsetAsync(ws, 0, align16(sizeof(double) * D) + align16(sizeof(uint32_t) * D), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(best, 0xff, 2 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
-    unsigned long long init[2] = {~0ull, ~0ull};
-    e = cudaMemcpyAsync(best_ws, init, sizeof(init), cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return e;
-    dim3 g((unsigned)((n + 1023) / 1024), (D + 127) / 128);
-    col_sum_kernel<<<g, 128, 0, st>>>(vecs, n, D, mean_ws);
-    medoid_dist_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(vecs, n, D, mean_ws, best_ws, 0);
-    medoid_dist_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(vecs, n, D, mean_ws, best_ws, 1);
-    return cudaGetLastError();
+    const dim3 g((unsigned)((n + 1023) / 1024), (D + 127) / 128);
+    col_bound_kernel<<<g, 128, 0, st>>>(vecs, n, D, bound);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    col_sum_kernel<<<g, 128, 0, st>>>(vecs, n, D, bound, B, sum);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    col_mean_kernel<<<(D + 127) / 128, 128, 0, st>>>(n, D, bound, B, sum);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const double* mean = reinterpret_cast<const double*>(sum);
+    for (int pass = 0; pass < 2; ++pass) {
+        medoid_dist_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(vecs, n, D, mean, best, pass);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (d_out != nullptr) {
+        medoid_result_kernel<<<1, 1, 0, st>>>(best, d_out);
+        e = cudaGetLastError();
+    }
+    return e;
 }
 
 // Reverse edges of a pruned batch: keys = target, vals = source, padded slots
@@ -268,15 +323,15 @@ cudaError_t launch_find_vectors(const float* vecs, uint64_t n, uint32_t D, const
 // hash set in shared memory (open addressing).  Distances are left to RobustPrune,
 // which computes them exactly.
 __global__ void consolidate_candidates_kernel(const uint32_t* deg, const uint32_t* adj, uint32_t R,
-                                              const uint32_t* tomb, uint64_t n, uint32_t* node_list,
-                                              uint32_t* n_list, uint32_t* cand, uint32_t* cand_n,
-                                              uint32_t cap, uint32_t hbits) {
+                                              const uint32_t* tomb, uint64_t first, uint64_t n,
+                                              uint32_t* node_list, uint32_t* n_list, uint32_t* cand,
+                                              uint32_t* cand_n, uint32_t cap, uint32_t hbits) {
     extern __shared__ uint32_t table_all[];
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t hs   = 1u << hbits;
     uint32_t*      tab  = table_all + (threadIdx.x >> 5) * hs;
     auto dead = [&](uint32_t id) { return (__ldg(tomb + (id >> 5)) >> (id & 31u)) & 1u; };
-    for (uint64_t p = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5); p < n;
+    for (uint64_t p = first + blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5); p < first + n;
          p += (uint64_t)gridDim.x * (blockDim.x / 32)) {
         if (dead((uint32_t)p)) continue;
         const uint32_t dg = min(deg[p], R);
@@ -347,7 +402,7 @@ __global__ void consolidate_candidates_kernel(const uint32_t* deg, const uint32_
     }
 }
 cudaError_t launch_consolidate_candidates(const uint32_t* deg, const uint32_t* adj, uint32_t R,
-                                          const uint32_t* tomb, uint64_t n, uint32_t* node_list,
+                                          const uint32_t* tomb, uint64_t first, uint64_t n, uint32_t* node_list,
                                           uint32_t* n_list, uint32_t* cand, uint32_t* cand_n, uint32_t cap,
                                           int num_sms, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
@@ -365,8 +420,9 @@ cudaError_t launch_consolidate_candidates(const uint32_t* deg, const uint32_t* a
     uint64_t grid = (uint64_t)per_sm * num_sms;
     const uint64_t need = (n + warps - 1) / warps;
     if (grid > need) grid = need;
-    consolidate_candidates_kernel<<<(unsigned)grid, warps * 32, smem, st>>>(deg, adj, R, tomb, n, node_list,
-                                                                            n_list, cand, cand_n, cap, hbits);
+    consolidate_candidates_kernel<<<(unsigned)grid, warps * 32, smem, st>>>(deg, adj, R, tomb, first, n,
+                                                                            node_list, n_list, cand, cand_n, cap,
+                                                                            hbits);
     return cudaGetLastError();
 }
 
@@ -374,22 +430,48 @@ cudaError_t launch_consolidate_candidates(const uint32_t* deg, const uint32_t* a
 
 // ---------------------------------------------------------------- allocation-free medoid
 // Entry-point selection (the medoid above) for callers that must not allocate
-// device memory.  Its scratch -- the D column sums (FP64) and the argmin word
-// pair -- lives in this file-scope device array instead of memory the library
-// would cudaMalloc: up to kNoAllocMaxDim dimensions, 32 KiB + 256 B, held by
-// every device that loads the library until the process exits.
+// device memory.  Its scratch -- per column a 64-bit sum (then the mean) and a
+// magnitude bound, and the argmin word pair -- lives in this file-scope device
+// array instead of memory the library would cudaMalloc: up to kNoAllocMaxDim
+// dimensions, 48 KiB + 256 B, held by every device that loads the library until
+// the process exits.
 namespace {
 constexpr uint32_t kNoAllocMaxDim = 4096;
-constexpr size_t   kNoAllocSumBytes = sizeof(double) * kNoAllocMaxDim;
-__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocSumBytes + 256];
+constexpr size_t   kNoAllocBytes  = 12 * (size_t)kNoAllocMaxDim + 256;
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-__global__ void medoid_result_kernel(const unsigned long long* best, uint32_t* out) {
-    *out = (uint32_t)best[1];
+// The device address of g_noalloc_scratch, resolved once per device and context:
+// in host code the symbol is only a stand-in.  A context created after a
+// cudaDeviceReset has its own copy of the array, so the address is resolved again
+// when the current context's id changes.
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+std::mutex         g_noalloc_mu;
+void*              g_noalloc_addr[256] = {};
+unsigned long long g_noalloc_ctx[256]  = {};
+CtxGetCurrentFn    g_ctx_current       = nullptr;
+CtxGetIdFn         g_ctx_id            = nullptr;
+bool               g_ctx_fns_looked_up = false;
+
+// id of the current context, 0 when it cannot be told (the address is then resolved on every call)
+unsigned long long current_context_id() {
+    if (!g_ctx_fns_looked_up) {
+        g_ctx_fns_looked_up = true;
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault) == cudaSuccess && f1 && f2) {
+            g_ctx_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+            g_ctx_id      = reinterpret_cast<CtxGetIdFn>(f2);
+        }
+        (void)cudaGetLastError();  // a failed lookup leaves no error behind for the caller
+    }
+    if (!g_ctx_current || !g_ctx_id) return 0;
+    void*              ctx = nullptr;
+    unsigned long long id  = 0;
+    if (g_ctx_current(&ctx) != 0 || ctx == nullptr || g_ctx_id(ctx, &id) != 0) return 0;
+    return id;
 }
-
-// device address of g_noalloc_scratch per device, resolved once per device
-std::mutex g_noalloc_mu;
-void*      g_noalloc_addr[256] = {};
 }  // namespace
 
 extern "C" vann_status vann_medoid_noalloc(const float* d_vecs, uint64_t n, uint32_t dim,
@@ -406,6 +488,14 @@ extern "C" vann_status vann_medoid_noalloc(const float* d_vecs, uint64_t n, uint
         vann::set_last_error("vann_medoid_noalloc: n must be below 2^32");
         return VANN_ERR_UNSUPPORTED;
     }
+    // an error left pending by earlier work is the caller's: report it as such,
+    // without consuming it, so the launch check below sees only this call's launches
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        vann::set_last_error((std::string("vann_medoid_noalloc: a CUDA error was already pending: ") +
+                              cudaGetErrorString(pending)).c_str());
+        return VANN_ERR_CUDA;
+    }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) {
         vann::set_last_error("vann_medoid_noalloc: no current CUDA device");
@@ -413,38 +503,30 @@ extern "C" vann_status vann_medoid_noalloc(const float* d_vecs, uint64_t n, uint
     }
     void* base = nullptr;
     {
-        // set-up on the first call on this device (with the device current):
-        // the host-side symbol is only a stand-in, the kernels need the device
-        // address, which cudaGetSymbolAddress resolves here
+        // set-up on the first call on this device (with the device current), and
+        // again in a new context: the kernels need the array's device address
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (g_noalloc_addr[dev] == nullptr) {
-            void* p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) {
-                vann::set_last_error("vann_medoid_noalloc: cudaGetSymbolAddress failed");
+        const unsigned long long ctx = current_context_id();
+        if (g_noalloc_addr[dev] == nullptr || ctx == 0 || ctx != g_noalloc_ctx[dev]) {
+            void*             p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || p == nullptr) {
+                vann::set_last_error((std::string("vann_medoid_noalloc: cudaGetSymbolAddress failed: ") +
+                                      cudaGetErrorString(e)).c_str());
                 return VANN_ERR_CUDA;
             }
             g_noalloc_addr[dev] = p;
+            g_noalloc_ctx[dev]  = ctx ? ctx : current_context_id();
         }
         base = g_noalloc_addr[dev];
     }
-    cudaStream_t        st   = static_cast<cudaStream_t>(stream);
-    double*             sums = static_cast<double*>(base);
-    unsigned long long* best = reinterpret_cast<unsigned long long*>(static_cast<char*>(base) + kNoAllocSumBytes);
-    // the array keeps the previous call's contents: clear what must start fresh
-    if (cudaMemsetAsync(sums, 0, sizeof(double) * dim, st) != cudaSuccess ||
-        cudaMemsetAsync(best, 0xff, 2 * sizeof(unsigned long long), st) != cudaSuccess) {
-        vann::set_last_error("vann_medoid_noalloc: clearing the scratch failed");
-        return VANN_ERR_CUDA;
-    }
-    dim3 g((unsigned)((n + 1023) / 1024), (dim + 127) / 128);
-    vann::col_sum_kernel<<<g, 128, 0, st>>>(d_vecs, n, dim, sums);
-    vann::medoid_dist_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_vecs, n, dim, sums, best, 0);
-    vann::medoid_dist_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_vecs, n, dim, sums, best, 1);
-    medoid_result_kernel<<<1, 1, 0, st>>>(best, d_medoid_out);
-    if (cudaGetLastError() != cudaSuccess) {
-        vann::set_last_error("vann_medoid_noalloc: kernel launch failed");
+    static_assert(12 * (size_t)kNoAllocMaxDim + 32 <= kNoAllocBytes, "scratch holds the medoid workspace");
+    // launch_medoid clears the sums, bounds and argmin pair the previous call left
+    const cudaError_t e =
+        vann::launch_medoid(d_vecs, n, dim, base, d_medoid_out, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) {
+        vann::set_last_error((std::string("vann_medoid_noalloc: ") + cudaGetErrorString(e)).c_str());
         return VANN_ERR_CUDA;
     }
     return VANN_OK;
 }
-

@@ -235,6 +235,7 @@ struct vann_index {
     // search order of large batches (distance keys, then the order), one workspace per
     // stream: searches in flight on different streams (the server's slots) never share it
     std::map<cudaStream_t, DevBuf> ord;
+    std::vector<void*>             ord_retired;  // outgrown order workspaces, freed at destroy
     DevBuf vis_ids, vis_d, vis_n, nodes, runs, ovf, stage, s2_ids, s2_d, e_keys, e_vals, e_keys2, e_vals2, counts, offsets, cub_tmp,
         medoid_ws, gather, cand, cand_n, list_n, out_tmp;
 
@@ -253,6 +254,7 @@ struct vann_index {
         cudaFree(counters);
         cudaFree(status);
         for (auto& o : ord) o.second.release();
+        for (void* r : ord_retired) cudaFree(r);
         for (DevBuf* b : {&vis_ids, &vis_d, &vis_n, &nodes, &runs, &ovf, &stage, &s2_ids, &s2_d, &e_keys, &e_vals, &e_keys2, &e_vals2,
                           &counts, &offsets, &cub_tmp, &medoid_ws, &gather, &cand, &cand_n,
                           &list_n, &out_tmp})
@@ -272,10 +274,27 @@ struct vann_index {
     // the queries farthest from the entry point first, since those tend to take the
     // most hops and, started last, would run on alone.  The order only changes which
     // warp runs a query when, never its result.
+    //
+    // A search captured into a CUDA graph keeps the address of this workspace, so a
+    // workspace that grows is retired (freed at vann_destroy), never freed while the
+    // index lives; and a search issued while its stream is being captured allocates
+    // nothing: when the stream's workspace is too small, that batch runs in input
+    // order, with the same results.
     const uint32_t* search_order(const float* d_queries, uint64_t nq, cudaStream_t st) {
         if (nq <= 16ull * (uint64_t)num_sms || nq > 0x7FFFFFFFull) return nullptr;
-        DevBuf& ob = ord[st];
-        ob.ensure(sizeof(uint32_t) * 2 * nq);
+        const size_t need = sizeof(uint32_t) * 2 * nq;
+        DevBuf&      ob   = ord[st];
+        if (ob.bytes < need) {
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            VCHECK(cudaStreamIsCapturing(st, &cs));
+            if (cs != cudaStreamCaptureStatusNone) return nullptr;
+            if (ob.p) {
+                ord_retired.push_back(ob.p);
+                ob.p     = nullptr;
+                ob.bytes = 0;
+            }
+            ob.ensure(need);
+        }
         uint32_t* keys  = ob.as<uint32_t>();
         uint32_t* order = keys + nq;
         entry_dist_kernel<<<(unsigned)((nq + 7) / 8), 256, 0, st>>>(d_queries, nq, p.dim,
@@ -372,14 +391,10 @@ struct vann_index {
     }
 
     uint32_t medoid(uint64_t n, cudaStream_t st) {
-        const size_t mean_bytes = (sizeof(double) * p.dim + 15) & ~size_t(15);
-        medoid_ws.ensure(mean_bytes + 16);
-        double*             mean = medoid_ws.as<double>();
-        unsigned long long* best =
-            reinterpret_cast<unsigned long long*>(static_cast<char*>(medoid_ws.p) + mean_bytes);
-        VCHECK(vann::launch_medoid(vecs, n, p.dim, mean, best, st));
+        medoid_ws.ensure(vann::medoid_ws_bytes(p.dim));
+        VCHECK(vann::launch_medoid(vecs, n, p.dim, medoid_ws.p, nullptr, st));
         unsigned long long hb[2];
-        VCHECK(cudaMemcpyAsync(hb, best, sizeof(hb), cudaMemcpyDeviceToHost, st));
+        VCHECK(cudaMemcpyAsync(hb, vann::medoid_best(medoid_ws.p, p.dim), sizeof(hb), cudaMemcpyDeviceToHost, st));
         VCHECK(cudaStreamSynchronize(st));
         return (uint32_t)hb[1];
     }
@@ -1244,40 +1259,51 @@ vann_status vann_consolidate(vann_index* h, void* stream) {
             return;
         }
         const uint32_t cap = std::min<uint32_t>(2048u, std::max<uint32_t>(h->p.max_visited, 2 * R));
-        h->nodes.ensure(sizeof(uint32_t) * h->size);
+        // Nodes go in ranges whose candidate lists fit a fixed workspace (cap words per
+        // node).  A node's candidates come from its own list and from deleted nodes'
+        // lists, which no prune of this call changes, so the ranges give the same
+        // graph as one pass over every node.
+        constexpr uint64_t kCandBudget = uint64_t(512) << 20;
+        const uint64_t     span = std::max<uint64_t>(1024, kCandBudget / (sizeof(uint32_t) * cap));
+        const uint64_t     rng  = std::min<uint64_t>(h->size, span);
+        h->nodes.ensure(sizeof(uint32_t) * rng);
         h->list_n.ensure(sizeof(uint32_t) * 4);
-        h->cand.ensure(sizeof(uint32_t) * h->size * cap);
-        h->cand_n.ensure(sizeof(uint32_t) * h->size);
-        VCHECK(cudaMemsetAsync(h->list_n.p, 0, sizeof(uint32_t), st));
-        VCHECK(vann::launch_consolidate_candidates(h->deg, h->adj, R, h->tomb, h->size,
-                                                   h->nodes.as<uint32_t>(), h->list_n.as<uint32_t>(),
-                                                   h->cand.as<uint32_t>(), h->cand_n.as<uint32_t>(), cap,
-                                                   h->num_sms, st));
-        uint32_t nlist = 0;
-        VCHECK(cudaMemcpyAsync(&nlist, h->list_n.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        VCHECK(cudaStreamSynchronize(st));
-        vann::PruneArgs pa{};
-        pa.vecs = h->vecs;
-        pa.D = h->p.dim;
-        pa.deg = h->deg;
-        pa.adj = h->adj;
-        pa.adj_h = h->adj_h;
-        pa.R = R;
-        pa.alpha = h->p.alpha;
-        pa.cap = cap;
-        pa.node_ids = h->nodes.as<uint32_t>();
-        pa.n_nodes = nlist;
-        pa.a_ids = h->cand.as<uint32_t>();
-        pa.a_d = nullptr;  // computed by the prune
-        pa.a_n = h->cand_n.as<uint32_t>();
-        pa.a_stride = cap;
-        pa.use_b = 0;
-        pa.consistent = 0;
-        pa.counter = h->next_counter(st);
-        pa.status = h->status;
-        h->run_prune(pa, st);
+        h->cand.ensure(sizeof(uint32_t) * rng * cap);
+        h->cand_n.ensure(sizeof(uint32_t) * rng);
+        for (uint64_t lo = 0; lo < h->size; lo += rng) {
+            const uint64_t cnt = std::min<uint64_t>(rng, h->size - lo);
+            VCHECK(cudaMemsetAsync(h->list_n.p, 0, sizeof(uint32_t), st));
+            VCHECK(vann::launch_consolidate_candidates(h->deg, h->adj, R, h->tomb, lo, cnt,
+                                                       h->nodes.as<uint32_t>(), h->list_n.as<uint32_t>(),
+                                                       h->cand.as<uint32_t>(), h->cand_n.as<uint32_t>(), cap,
+                                                       h->num_sms, st));
+            uint32_t nlist = 0;
+            VCHECK(cudaMemcpyAsync(&nlist, h->list_n.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            VCHECK(cudaStreamSynchronize(st));
+            if (nlist == 0) continue;
+            vann::PruneArgs pa{};
+            pa.vecs = h->vecs;
+            pa.D = h->p.dim;
+            pa.deg = h->deg;
+            pa.adj = h->adj;
+            pa.adj_h = h->adj_h;
+            pa.R = R;
+            pa.alpha = h->p.alpha;
+            pa.cap = cap;
+            pa.node_ids = h->nodes.as<uint32_t>();
+            pa.n_nodes = nlist;
+            pa.a_ids = h->cand.as<uint32_t>();
+            pa.a_d = nullptr;  // computed by the prune
+            pa.a_n = h->cand_n.as<uint32_t>();
+            pa.a_stride = cap;
+            pa.use_b = 0;
+            pa.consistent = 0;
+            pa.counter = h->next_counter(st);
+            pa.status = h->status;
+            h->run_prune(pa, st);
+        }
         // free the deleted ids (tombstone stays set until an insert reuses the id)
-        h->nodes.ensure(sizeof(uint32_t) * std::max<size_t>(dead.size(), h->size));
+        h->nodes.ensure(sizeof(uint32_t) * dead.size());
         VCHECK(cudaMemcpyAsync(h->nodes.p, dead.data(), sizeof(uint32_t) * dead.size(),
                                cudaMemcpyHostToDevice, st));
         clear_deg_kernel<<<(unsigned)((dead.size() + 255) / 256), 256, 0, st>>>(

@@ -129,15 +129,19 @@ cudaError_t launch_convert_ids(const float* vecs, const uint32_t* ids, uint64_t 
 cudaError_t launch_iota(uint32_t* out, uint64_t n, uint32_t first, cudaStream_t st);
 cudaError_t launch_set_bits(uint32_t* bits, const uint32_t* ids, uint64_t n, uint64_t limit,
                             cudaStream_t st);
-cudaError_t launch_medoid(const float* vecs, uint64_t n, uint32_t D, double* mean_ws,
-                          unsigned long long* best_ws, cudaStream_t st);
+// Medoid of rows 0 .. n-1 into ws (medoid_ws_bytes(D) bytes); the id ends in
+// medoid_best(ws, D)[1] and, when d_out is set, in *d_out.  Allocates nothing.
+size_t              medoid_ws_bytes(uint32_t D);
+unsigned long long* medoid_best(void* ws, uint32_t D);
+cudaError_t launch_medoid(const float* vecs, uint64_t n, uint32_t D, void* ws, uint32_t* d_out, cudaStream_t st);
 cudaError_t launch_edges(const uint32_t* nodes, uint64_t n_nodes, const uint32_t* deg,
                          const uint32_t* adj, uint32_t R, uint32_t* keys, uint32_t* vals,
                          uint32_t* counts, cudaStream_t st);
 cudaError_t launch_find_vectors(const float* vecs, uint64_t n, uint32_t D, const float* q,
                                 uint64_t nq, const uint32_t* tomb, int32_t* out, cudaStream_t st);
+// candidate lists of the live nodes first .. first+n-1 that have a deleted neighbour
 cudaError_t launch_consolidate_candidates(const uint32_t* deg, const uint32_t* adj, uint32_t R,
-                                          const uint32_t* tomb, uint64_t n, uint32_t* node_list,
+                                          const uint32_t* tomb, uint64_t first, uint64_t n, uint32_t* node_list,
                                           uint32_t* n_list, uint32_t* cand, uint32_t* cand_n, uint32_t cap,
                                           int num_sms, cudaStream_t st);
 

@@ -289,18 +289,22 @@ vann_status vann_server_get_stats(vann_server* server, vann_server_stats* out);
  * of d_vecs of the FP64 squared distance to their mean, smallest id on ties --
  * the same value vann_build picks) into *d_medoid_out, without allocating any
  * device memory: its scratch is a fixed device array inside libvann.so
- * (32 KiB + 256 B, kept by every device that loads the library until exit).
- * For callers that cannot call cudaMalloc/cudaFree: code issuing work while a
- * stream is being captured into a CUDA graph, processes whose device memory is
- * owned by another allocator, and latency-bound threads that must not take the
- * allocator's locks or the device synchronisation that cudaFree implies.
+ * (48 KiB + 256 B, kept by every device that loads the library until exit).
+ * For callers that cannot call cudaMalloc/cudaFree: processes whose device
+ * memory is owned by another allocator under a fixed budget, threads on a
+ * latency-critical path that must not take the allocator's locks or the device
+ * synchronisation that cudaFree implies, and code that must not meet an
+ * allocation failure at call time.
  * Limits: dim <= 4096 (larger returns VANN_ERR_UNSUPPORTED), n < 2^32.
- * Asynchronous on `stream`.  The first call on a device resolves the array's
- * device address, so make it before any stream capture.  Each device has one
- * such array and every call on that device shares it, keeping the previous
- * call's contents until the next call clears it: calls on one device that
- * overlap on the GPU (e.g. issued on different streams) race on it, so
- * serialise them. */
+ * Asynchronous on `stream`.  The column sums are exact (fixed-point integer
+ * sums), so the result does not depend on the order of the device's additions.
+ * The first call on a device (and the first in a context created after a
+ * cudaDeviceReset) resolves the array's device address; make it before any
+ * stream capture.  A CUDA error already pending when the call is made is
+ * reported (VANN_ERR_CUDA) and left pending.  Each device has one such array
+ * and every call on that device shares it, keeping the previous call's contents
+ * until the next call clears it: calls on one device that overlap on the GPU
+ * (e.g. issued on different streams) race on it, so serialise them. */
 vann_status vann_medoid_noalloc(const float* d_vecs, uint64_t n, uint32_t dim, uint32_t* d_medoid_out,
                                 void* stream);
 

@@ -53,17 +53,20 @@ def lib():
         L.vo_search_batch.restype = C.c_int
         L.vo_search_batch.argtypes = [C.POINTER(_Graph), C.c_void_p, C.c_int64, C.c_int, C.c_int,
                                       C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
-                                      C.c_void_p, C.c_void_p, C.c_int]
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.vo_search_one.restype = C.c_int
         L.vo_search_one.argtypes = [C.POINTER(_Graph), C.c_void_p, C.c_int, C.c_uint32, C.c_uint32,
                                     C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
-                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.vo_robust_prune.restype = C.c_int
         L.vo_robust_prune.argtypes = [C.POINTER(_Graph), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                       C.c_float, C.c_int, C.c_void_p, C.c_void_p]
         L.vo_vamana_batch.restype = C.c_int
         L.vo_vamana_batch.argtypes = [C.POINTER(_Graph), C.c_int64, C.c_int64, C.c_int, C.c_float,
                                       C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.vo_consolidate.restype = C.c_int
+        L.vo_consolidate.argtypes = [C.POINTER(_Graph), C.c_float, C.c_int, C.c_void_p, C.c_uint32,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.vo_random_graph.restype = None
         L.vo_random_graph.argtypes = [C.c_int64, C.c_int, C.c_uint64, C.c_void_p, C.c_void_p]
         L.vo_bruteforce_knn.restype = None
@@ -101,17 +104,20 @@ class Graph:
         return _Graph(_p(self.vecs), self.n, self.vecs.shape[1], _p(self.deg), _p(self.adj), self.R,
                       _p(self.tomb))
 
-    def search(self, q, L, k, entry, skip_mode=0, bloom_mode=BLOOM_CHUNK32, max_hops=1 << 30, threads=0):
+    def search(self, q, L, k, entry, skip_mode=0, bloom_mode=BLOOM_CHUNK32, max_hops=1 << 30, threads=0,
+               with_adjw=False):
+        """-> status, ids, dists, hops, evals (and with_adjw the adjacency words read)."""
         q = np.ascontiguousarray(q, dtype=np.float32)
         nq = q.shape[0]
         ids = np.empty((nq, k), np.uint32)
         d = np.empty((nq, k), np.float32)
         hops = np.empty(nq, np.int32)
         evals = np.empty(nq, np.int64)
+        adjw = np.empty(nq, np.int64)
         g = self._c()
         st = lib().vo_search_batch(C.byref(g), _p(q), nq, L, k, entry, skip_mode, bloom_mode, max_hops,
-                                   _p(ids), _p(d), _p(hops), _p(evals), threads)
-        return st, ids, d, hops, evals
+                                   _p(ids), _p(d), _p(hops), _p(evals), _p(adjw), threads)
+        return (st, ids, d, hops, evals, adjw) if with_adjw else (st, ids, d, hops, evals)
 
     def search_one(self, q, L, entry, skip_id=NONE, bloom_mode=BLOOM_CHUNK32, max_visited=600,
                    max_hops=1 << 30):
@@ -127,7 +133,7 @@ class Graph:
         g = self._c()
         st = lib().vo_search_one(C.byref(g), _p(q), L, entry, skip_id, bloom_mode, max_visited, max_hops,
                                  _p(wi), _p(wd), C.byref(wn), _p(vi), _p(vd), C.byref(vn), C.byref(hops),
-                                 C.byref(ev))
+                                 C.byref(ev), None)
         return st, wi[: wn.value], wd[: wn.value], vi[: vn.value], vd[: vn.value], hops.value, ev.value
 
     def robust_prune(self, node_vec, cand, cand_d, alpha, R):
@@ -139,11 +145,33 @@ class Graph:
         d = lib().vo_robust_prune(C.byref(g), _p(nv), _p(cand), _p(cand_d), len(cand), alpha, R, _p(out), None)
         return out[:d]
 
+    def consolidate(self, alpha, cap, entry, is_free=None, threads=0):
+        """FreshVamana delete consolidation of the ids marked in self.tomb (vo_consolidate):
+        updates deg/adj in place; -> (new entry, ids freed by this call, ascending)."""
+        assert self.tomb is not None
+        g = self._c()
+        free_mask = None if is_free is None else np.ascontiguousarray(is_free, dtype=np.uint8)
+        freed = np.empty(max(self.n, 1), np.uint32)
+        nf = C.c_int64(0)
+        ne = C.c_uint32(0)
+        st = lib().vo_consolidate(C.byref(g), alpha, cap, _p(free_mask), entry, C.byref(ne), _p(freed),
+                                  C.byref(nf), threads)
+        assert st == 0, st
+        return int(ne.value), freed[: nf.value].copy()
+
     def vamana_batch(self, batch_start, batch_n, L, alpha, entry, max_visited=600, max_reverse=500,
                      skip_mode=1, bloom_mode=BLOOM_CHUNK32, threads=0):
         g = self._c()
         return lib().vo_vamana_batch(C.byref(g), batch_start, batch_n, L, alpha, entry, max_visited,
                                      max_reverse, skip_mode, bloom_mode, threads)
+
+
+def tomb_bitmap(n: int, ids) -> np.ndarray:
+    """Tombstone bitmap of n ids (bit i of word i >> 5) with `ids` set."""
+    t = np.zeros((n + 31) // 32, np.uint32)
+    for i in np.asarray(ids, dtype=np.int64).tolist():
+        t[i >> 5] |= np.uint32(1 << (i & 31))
+    return t
 
 
 def bf_h1(x: int) -> int:

@@ -75,7 +75,7 @@ static int cmp_dist_pos(const void* a, const void* b) {
 int vo_search_one(const vo_graph* g, const float* q, int L, uint32_t entry, uint32_t skip_id,
                   int bloom_mode, int max_visited, int max_hops, uint32_t* wl_ids, float* wl_d,
                   int* wl_n, uint32_t* vis_ids, float* vis_d, int* vis_n, int* hops_out,
-                  int64_t* evals_out) {
+                  int64_t* evals_out, int64_t* adjw_out) {
     const int     D   = g->dim;
     const int     R   = g->R;
     unsigned char* bf = (unsigned char*)calloc(VO_BF_ENTRIES, 1);
@@ -98,6 +98,7 @@ int vo_search_one(const vo_graph* g, const float* q, int L, uint32_t entry, uint
     float    parent_d = wl_d[0];
     int      hops     = 0;
     int      nv       = 0;
+    int64_t  adjw     = 0;
 
     for (;;) {
         if (hops >= max_hops) {
@@ -113,8 +114,9 @@ int vo_search_one(const vo_graph* g, const float* q, int L, uint32_t entry, uint
             if (vis_d) vis_d[nv] = parent_d;
             ++nv;
         }
-        const uint32_t  deg = g->deg[parent];
+        const uint32_t  deg = g->deg[parent] < (uint32_t)R ? g->deg[parent] : (uint32_t)R;
         const uint32_t* row = g->adj + (size_t)parent * R;
+        adjw += deg;
         int             cnt = 0;
         const uint32_t  chunk = bloom_mode == VO_BLOOM_SEQUENTIAL ? 1u
                                 : bloom_mode == VO_BLOOM_SNAPSHOT ? (deg ? deg : 1u)
@@ -181,6 +183,7 @@ int vo_search_one(const vo_graph* g, const float* q, int L, uint32_t entry, uint
     if (vis_n) *vis_n = nv;
     if (hops_out) *hops_out = hops;
     if (evals_out) *evals_out = evals;
+    if (adjw_out) *adjw_out = adjw;
     free(bf);
     free(wl_v);
     free(nb);
@@ -193,7 +196,7 @@ int vo_search_one(const vo_graph* g, const float* q, int L, uint32_t entry, uint
 
 int vo_search_batch(const vo_graph* g, const float* q, int64_t nq, int L, int k, uint32_t entry,
                     int skip_mode, int bloom_mode, int max_hops, uint32_t* out_ids, float* out_d,
-                    int32_t* hops, int64_t* evals, int threads) {
+                    int32_t* hops, int64_t* evals, int64_t* adjw, int threads) {
     if (L < 1 || k < 1 || k > L || g->R > 64 * 1024) return VO_ERR_INVALID;
     int status = VO_OK;
     if (threads <= 0) threads = omp_get_max_threads();
@@ -204,10 +207,10 @@ int vo_search_batch(const vo_graph* g, const float* q, int64_t nq, int L, int k,
 #pragma omp for schedule(dynamic, 16)
         for (int64_t s = 0; s < nq; ++s) {
             int      wn = 0, h = 0;
-            int64_t  e  = 0;
+            int64_t  e = 0, aw = 0;
             uint32_t skip = skip_mode == 1 ? (uint32_t)s : VO_NONE;
             int st = vo_search_one(g, q + (size_t)s * g->dim, L, entry, skip, bloom_mode, 0,
-                                   max_hops, wi, wd, &wn, NULL, NULL, NULL, &h, &e);
+                                   max_hops, wi, wd, &wn, NULL, NULL, NULL, &h, &e, &aw);
             if (st != VO_OK) {
 #pragma omp atomic write
                 status = st;
@@ -218,6 +221,7 @@ int vo_search_batch(const vo_graph* g, const float* q, int64_t nq, int L, int k,
             }
             if (hops) hops[s] = h;
             if (evals) evals[s] = e;
+            if (adjw) adjw[s] = aw;
         }
         free(wi);
         free(wd);
@@ -322,7 +326,7 @@ int vo_vamana_batch(vo_graph* g, int64_t batch_start, int64_t batch_n, int L, fl
             int wn = 0;
             int st = vo_search_one(g, g->vecs + (size_t)node * D, L, entry, skip, bloom_mode,
                                    max_visited, 1 << 30, wi, wd, &wn, vis + (size_t)b * max_visited,
-                                   vis_d + (size_t)b * max_visited, &vis_n[b], NULL, NULL);
+                                   vis_d + (size_t)b * max_visited, &vis_n[b], NULL, NULL, NULL);
             if (st != VO_OK) {
 #pragma omp atomic write
                 status = st;
@@ -563,4 +567,123 @@ void vo_merge_rerank(const float* vecs, int dim, const float* q, int64_t nq, con
                     sid[j + 1]  = ti;
                 }
     }
+}
+
+/* ---------------------------------------------------------------- delete consolidation
+ * The reference never consolidates deletes: patchGraph (vamana_impl.cuh:182-265)
+ * folds in inserts only, and deleted ids stay behind a delete list that every
+ * search scans (search.cuh:121-123, delete_list.cuh:108-115).  FreshVamana's
+ * consolidation is the published FreshDiskANN rule (Singh, Subramanya,
+ * Krishnaswamy, Simhadri, "FreshDiskANN", 2021, Algorithm 4 "Delete"):
+ *   for every live p with N_out(p) meeting the deleted set D:
+ *     C = (N_out(p) \ D)  U  (U_{v in N_out(p) & D} N_out(v)),  minus D and p;
+ *     N_out(p) = RobustPrune(p, C, alpha, R).
+ * The paper leaves the order of C open.  This restatement fixes the order the
+ * engine uses: p's list in its order, each deleted neighbour replaced where it
+ * stands by its own out-neighbours in their order, repeats dropped (the first
+ * occurrence stays), at most `cap` entries.  Distances to p are FP32 (vo_l2sq),
+ * the list is sorted stably by distance and pruned with vo_robust_prune.  Every
+ * candidate list is taken from the graph before any node is re-pruned.
+ * Then the deleted ids that are not free yet get degree 0 and join the free
+ * list in ascending order; a deleted entry point moves to the first live id in
+ * the L = 32 worklist of a search for its vector, started at the lowest live
+ * id, over the consolidated graph (the tombstones stay set).
+ * g->tomb marks the deleted ids; is_free (n bytes, may be NULL) marks ids
+ * freed by an earlier consolidation. */
+int vo_consolidate(vo_graph* g, float alpha, int cap, const unsigned char* is_free, uint32_t entry,
+                   uint32_t* new_entry, uint32_t* freed, int64_t* n_freed, int threads) {
+    const int     R = g->R, D = g->dim;
+    const int64_t N = g->n;
+    if (!g->tomb || cap < 1 || R < 1) return VO_ERR_INVALID;
+    if (threads <= 0) threads = omp_get_max_threads();
+    uint32_t* new_adj = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(N ? N : 1) * R);
+    int32_t*  new_deg = (int32_t*)malloc(sizeof(int32_t) * (size_t)(N ? N : 1));
+#pragma omp parallel num_threads(threads)
+    {
+        uint32_t* seen = (uint32_t*)calloc((size_t)(N ? N : 1), sizeof(uint32_t));
+        vo_item*  it   = (vo_item*)malloc(sizeof(vo_item) * (size_t)cap);
+        uint32_t* ci   = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)cap);
+        float*    cd   = (float*)malloc(sizeof(float) * (size_t)cap);
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t p = 0; p < N; ++p) {
+            new_deg[p] = -1; /* unchanged */
+            if (tomb_get(g->tomb, (uint32_t)p)) continue;
+            const uint32_t  dp  = g->deg[p] < (uint32_t)R ? g->deg[p] : (uint32_t)R;
+            const uint32_t* row = g->adj + (size_t)p * R;
+            int             any = 0;
+            for (uint32_t j = 0; j < dp && !any; ++j) any = tomb_get(g->tomb, row[j]);
+            if (!any) continue;
+            const uint32_t stamp = (uint32_t)p + 1u;
+            int            nc    = 0;
+#define VO_PUSH(u)                                                                  \
+    do {                                                                            \
+        uint32_t u_ = (u);                                                          \
+        if (nc < cap && u_ != (uint32_t)p && !tomb_get(g->tomb, u_) && seen[u_] != stamp) { \
+            seen[u_]   = stamp;                                                     \
+            it[nc].id  = u_;                                                        \
+            it[nc].pos = (uint32_t)nc;                                              \
+            ++nc;                                                                   \
+        }                                                                           \
+    } while (0)
+            for (uint32_t j = 0; j < dp && nc < cap; ++j) {
+                const uint32_t v = row[j];
+                if (!tomb_get(g->tomb, v)) {
+                    VO_PUSH(v);
+                } else {
+                    const uint32_t  dv   = g->deg[v] < (uint32_t)R ? g->deg[v] : (uint32_t)R;
+                    const uint32_t* rowv = g->adj + (size_t)v * R;
+                    for (uint32_t t = 0; t < dv && nc < cap; ++t) VO_PUSH(rowv[t]);
+                }
+            }
+#undef VO_PUSH
+            const float* pv = g->vecs + (size_t)p * D;
+            for (int t = 0; t < nc; ++t) it[t].d = vo_l2sq(pv, g->vecs + (size_t)it[t].id * D, D);
+            qsort(it, (size_t)nc, sizeof(vo_item), cmp_dist_pos);
+            for (int t = 0; t < nc; ++t) {
+                ci[t] = it[t].id;
+                cd[t] = it[t].d;
+            }
+            new_deg[p] = vo_robust_prune(g, pv, ci, cd, nc, alpha, R, new_adj + (size_t)p * R, NULL);
+        }
+        free(seen);
+        free(it);
+        free(ci);
+        free(cd);
+    }
+    int64_t nf = 0;
+    for (int64_t p = 0; p < N; ++p) {
+        if (new_deg[p] >= 0) {
+            g->deg[p] = (uint32_t)new_deg[p];
+            memcpy(g->adj + (size_t)p * R, new_adj + (size_t)p * R, sizeof(uint32_t) * (size_t)new_deg[p]);
+        }
+        if (tomb_get(g->tomb, (uint32_t)p) && !(is_free && is_free[p])) {
+            g->deg[p] = 0;
+            if (freed) freed[nf] = (uint32_t)p;
+            ++nf;
+        }
+    }
+    free(new_adj);
+    free(new_deg);
+    if (n_freed) *n_freed = nf;
+    uint32_t ne = entry;
+    if (entry < (uint64_t)N && tomb_get(g->tomb, entry)) {
+        uint32_t start = VO_NONE;
+        for (int64_t i = 0; i < N && start == VO_NONE; ++i)
+            if (!tomb_get(g->tomb, (uint32_t)i)) start = (uint32_t)i;
+        if (start == VO_NONE) return VO_ERR_INVALID;
+        uint32_t wi[32];
+        float    wd[32];
+        int      wn = 0;
+        int st = vo_search_one(g, g->vecs + (size_t)entry * D, 32, start, VO_NONE, VO_BLOOM_SNAPSHOT, 0,
+                               1 << 30, wi, wd, &wn, NULL, NULL, NULL, NULL, NULL, NULL);
+        if (st != VO_OK) return st;
+        ne = start;
+        for (int t = 0; t < wn; ++t)
+            if (!tomb_get(g->tomb, wi[t])) {
+                ne = wi[t];
+                break;
+            }
+    }
+    if (new_entry) *new_entry = ne;
+    return VO_OK;
 }

@@ -59,14 +59,15 @@ float    vo_l2sq(const float* a, const float* b, int dim);
 int vo_search_one(const vo_graph* g, const float* q, int L, uint32_t entry, uint32_t skip_id,
                   int bloom_mode, int max_visited, int max_hops, uint32_t* wl_ids, float* wl_d,
                   int* wl_n, uint32_t* vis_ids, float* vis_d, int* vis_n, int* hops,
-                  int64_t* evals);
+                  int64_t* evals, int64_t* adjw);
 
 /* Batched search: out_ids/out_d are n x k (padded with VO_NONE / +inf).
  * skip_mode: 0 = no skip, 1 = skip the query's batch index (reference quirk
- * search.cuh:126).  hops/evals may be NULL.  threads <= 0 means all cores. */
+ * search.cuh:126).  hops/evals/adjw may be NULL; adjw counts the adjacency words
+ * read (the sum of the expanded parents' degrees).  threads <= 0 means all cores. */
 int vo_search_batch(const vo_graph* g, const float* q, int64_t nq, int L, int k, uint32_t entry,
                     int skip_mode, int bloom_mode, int max_hops, uint32_t* out_ids, float* out_d,
-                    int32_t* hops, int64_t* evals, int threads);
+                    int32_t* hops, int64_t* evals, int64_t* adjw, int threads);
 
 /* RobustPrune over a sorted candidate list (kernels.cuh:232-356).  Returns the
  * new degree; writes the chosen ids in selection order to out. */
@@ -83,6 +84,14 @@ int vo_robust_prune(const vo_graph* g, const float* node_vec, const uint32_t* ca
 int vo_vamana_batch(vo_graph* g, int64_t batch_start, int64_t batch_n, int L, float alpha,
                     uint32_t entry, int max_visited, int max_reverse, int skip_mode,
                     int bloom_mode, int threads);
+
+/* FreshVamana delete consolidation (FreshDiskANN, Singh et al. 2021, Algorithm 4)
+ * over the ids marked in g->tomb; the candidate order is fixed as described in
+ * vann_oracle.c.  g->deg / g->adj are updated in place; the ids freed by this call
+ * (deleted and not marked in is_free) are written ascending to `freed` (n entries
+ * at most) and counted in n_freed; new_entry is the entry point afterwards. */
+int vo_consolidate(vo_graph* g, float alpha, int cap, const unsigned char* is_free, uint32_t entry,
+                   uint32_t* new_entry, uint32_t* freed, int64_t* n_freed, int threads);
 
 /* Deterministic random initial graph (hash-based, no self loops). */
 void vo_random_graph(int64_t n, int R, uint64_t seed, uint32_t* deg, uint32_t* adj);

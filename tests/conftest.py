@@ -9,7 +9,8 @@ for p in (ROOT, PKG):
     if p not in sys.path:
         sys.path.insert(0, p)
 
-REFERENCE = "/root/reference"
+# the reference checkout (read only by the golden-file tests); absent on a GPU box
+REFERENCE = os.environ.get("VANN_REFERENCE_DIR", "/root/reference")
 
 
 def pytest_configure(config):

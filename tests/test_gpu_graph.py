@@ -39,3 +39,48 @@ def test_captured_search_replays_exactly(vann_mod, store, L, rerank, beam):
         torch.cuda.synchronize()
         assert torch.equal(out[0], want[i][0]) and torch.equal(out[1], want[i][1]), i
     del g
+
+
+def test_captured_large_batches(vann_mod):
+    """Batches above 16 queries per SM use the order workspace.  Captured without an
+    uncaptured call on the capture stream first, the search allocates nothing and runs
+    in input order; after a warm-up on that stream it captures the ordered search.  A
+    later, larger uncaptured search on the same stream grows the workspace without
+    freeing the one the graph holds.  Every replay equals the direct call."""
+    import torch
+
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+    nq = 16 * nsm + 700
+    base = workload.mixture(5000, 128, 30, seed=141)
+    idx = vann_mod.Index(128, 32, 64, 1.2, capacity=5000, stores=("f32", "u8"))
+    idx.build(torch.from_numpy(base).cuda(), batch=0, seed=2)
+    batches = [torch.from_numpy(workload.mixture(nq, 128, 30, seed=142 + i)).cuda() for i in range(2)]
+    want = [idx.search(b, k=10, L=32, store="u8") for b in batches]
+    torch.cuda.synchronize()
+    q = batches[0].clone()
+    out = (torch.empty((nq, 10), dtype=torch.int32, device="cuda"),
+           torch.empty((nq, 10), dtype=torch.float32, device="cuda"))
+    big = torch.from_numpy(workload.mixture(4 * nq, 128, 30, seed=149)).cuda()
+    graphs = []
+    for warm in (False, True):
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        if warm:
+            with torch.cuda.stream(s):
+                idx.search(q, k=10, L=32, store="u8", out=out)
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            idx.search(q, k=10, L=32, store="u8", out=out)
+        with torch.cuda.stream(s):
+            idx.search(big, k=10, L=32, store="u8")  # grows this stream's workspace
+        torch.cuda.synchronize()
+        graphs.append(g)
+    for g in graphs:
+        for i, b in enumerate(batches):
+            q.copy_(b)
+            g.replay()
+            torch.cuda.synchronize()
+            assert torch.equal(out[0], want[i][0]) and torch.equal(out[1], want[i][1]), i
+    del graphs

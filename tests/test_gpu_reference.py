@@ -51,8 +51,9 @@ def test_search_matches_reference_cuda(oracle, vann_mod, tmp_path):
 
     exact = (ours == ref_ids).all(axis=1)
     assert exact.mean() >= 0.95, exact.mean()
-    # where a query differs, the distance sequences still agree: only tied ids moved
+    # where a query differs, the whole L-long distance sequences still agree: only
+    # tied ids moved
     for s in np.where(~exact)[0]:
         da = ((base[ours[s]].astype(np.float64) - q[s]) ** 2).sum(1)
         db = ((base[ref_ids[s]].astype(np.float64) - q[s]) ** 2).sum(1)
-        assert np.array_equal(da[:10], db[:10])
+        assert np.array_equal(da, db), s

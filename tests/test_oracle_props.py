@@ -141,3 +141,39 @@ def test_merge_rerank_matches_the_reference_loop(oracle):
     assert np.array_equal(ids, ri)
     assert np.array_equal(d, rd)
     assert (ids >= oracle.STAGED).any() and (ids < oracle.STAGED).any()
+
+
+def test_consolidate_properties(oracle, small):
+    """The oracle's delete consolidation (FreshDiskANN Algorithm 4): no live node
+    keeps a deleted neighbour, every list stays a RobustPrune output (no repeats,
+    degree <= R), the deleted ids are freed with degree 0, a deleted entry moves to
+    a live node, the result does not depend on the thread count, and the lists of
+    nodes without a deleted neighbour are untouched.  Recall over the live rows
+    stays high."""
+    base, q = small
+    n = base.shape[0]
+    g0, entry = oracle.build_index(base, R=32, L=75, alpha=1.2, seed=5)
+    rng = np.random.default_rng(4)
+    dead = np.unique(np.append(rng.choice(n, 300, replace=False), entry))
+    tomb = oracle.tomb_bitmap(n, dead)
+    a = oracle.Graph(base, g0.deg.copy(), g0.adj.copy(), tomb=tomb)
+    b = oracle.Graph(base, g0.deg.copy(), g0.adj.copy(), tomb=tomb.copy())
+    ea, fa = a.consolidate(1.2, 600, entry, threads=1)
+    eb, fb = b.consolidate(1.2, 600, entry, threads=8)
+    assert ea == eb and np.array_equal(fa, fb) and np.array_equal(a.deg, b.deg)
+    assert np.array_equal(fa, np.sort(dead).astype(np.uint32))
+    dead_set = set(dead.tolist())
+    assert ea not in dead_set
+    for i in range(n):
+        row = a.adj[i, :a.deg[i]]
+        assert np.array_equal(a.adj[i, :a.deg[i]], b.adj[i, :b.deg[i]])
+        if i in dead_set:
+            assert a.deg[i] == 0
+            continue
+        assert not (set(row.tolist()) & dead_set) and len(set(row.tolist())) == len(row) and len(row) <= 32
+        if not (set(g0.adj[i, :g0.deg[i]].tolist()) & dead_set):
+            assert np.array_equal(row, g0.adj[i, :g0.deg[i]])
+    live = np.array(sorted(set(range(n)) - dead_set))
+    truth, _ = oracle.bruteforce_knn(base[live], q, 10)
+    st, ids, _, _, _ = a.search(q, 75, 10, ea)
+    assert st == 0 and oracle.recall_at_k(ids, live[truth], 10) >= 0.95
