@@ -372,19 +372,21 @@ def main():
         traffic = None
 
     # ---- e2e through the public API with pinned host buffers.  Each step copies
-    # its queries host->device, searches and copies ids/distances back; steps are
-    # double-buffered so one step's copies overlap its neighbours' searches (an
-    # upload stream and a download stream beside the compute stream), as a
-    # serving pipeline would run.
+    # its queries host->device, searches and copies ids/distances back.  Steps are
+    # pipelined as a serving loop runs them: an upload stream, two compute streams
+    # taking the steps in turn, and a download stream, so one step's copies overlap
+    # its neighbours' searches and the tail of one search (its last, longest
+    # queries) overlaps the start of the next.
     _, hs, hrr, hbeam = form_of[head]
     h_q = torch.from_numpy(q).pin_memory()
-    s_comp = torch.cuda.current_stream()
+    s_comp = [torch.cuda.Stream(), torch.cuda.Stream()]
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
     qbuf = [torch.empty_like(q_d) for _ in range(2)]
     obuf = [(torch.empty((nq, K), dtype=torch.int32, device=dev),
              torch.empty((nq, K), dtype=torch.float32, device=dev)) for _ in range(2)]
     h_out = [(torch.empty((nq, K), dtype=torch.int32).pin_memory(),
               torch.empty((nq, K), dtype=torch.float32).pin_memory()) for _ in range(2)]
+    flushes = [flush, torch.empty_like(flush)]
     ev_in = [torch.cuda.Event() for _ in range(2)]
     ev_done = [torch.cuda.Event() for _ in range(2)]
     ev_out = [torch.cuda.Event() for _ in range(2)]
@@ -392,18 +394,19 @@ def main():
     def e2e_run(nsteps):
         for i in range(nsteps):
             bsel = i % 2
+            sc = s_comp[bsel]
             with torch.cuda.stream(s_in):
                 if i >= 2:
                     s_in.wait_event(ev_done[bsel])  # the search that read this buffer
                 qbuf[bsel].copy_(h_q, non_blocking=True)
                 ev_in[bsel].record(s_in)
-            s_comp.wait_event(ev_in[bsel])
+            sc.wait_event(ev_in[bsel])
             if i >= 2:
-                s_comp.wait_event(ev_out[bsel])  # the download of this buffer's last results
-            with torch.cuda.stream(s_comp):
-                flush.zero_()  # L2 flushed before every search, as in the device-timed loop
-            idx.search(qbuf[bsel], k=K, L=hr["L"], store=hs, rerank=hrr, out=obuf[bsel], stream=s_comp, beam=hbeam)
-            ev_done[bsel].record(s_comp)
+                sc.wait_event(ev_out[bsel])  # the download of this buffer's last results
+            with torch.cuda.stream(sc):
+                flushes[bsel].zero_()  # an L2 flush (256 MB write) before every search
+            idx.search(qbuf[bsel], k=K, L=hr["L"], store=hs, rerank=hrr, out=obuf[bsel], stream=sc, beam=hbeam)
+            ev_done[bsel].record(sc)
             with torch.cuda.stream(s_out):
                 s_out.wait_event(ev_done[bsel])
                 h_out[bsel][0].copy_(obuf[bsel][0], non_blocking=True)
@@ -483,7 +486,9 @@ def main():
             "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": nq * DIM * 4,
                     "d2h_bytes_per_step": nq * K * 8,
                     "how": "C ABI search on pinned host queries; per step H2D + L2 flush (256 MB write) + "
-                           "search + D2H, double-buffered on upload, compute and download streams"},
+                           "search + D2H; steps pipelined on an upload stream, two compute streams taking "
+                           "the steps in turn, and a download stream (a step's tail overlaps the next "
+                           "step's start, as in a serving loop)"},
             # per step: the search, and for a batch over 16 queries per SM the two kernels
             # that order it (entry distances, bucket order)
             "gpu_launches": steps * (3 if nq > 16 * torch.cuda.get_device_properties(dev).multi_processor_count

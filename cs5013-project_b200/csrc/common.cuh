@@ -3,7 +3,7 @@
 // Data layout in HBM (one index):
 //   vecs_f32  [capacity x D]  FP32 rows, 16-byte aligned (D % 4 == 0)
 //   vecs_bf16 [capacity x D]  optional traversal copy
-//   vecs_fp8  [capacity x D]  optional e4m3 copy + scale_fp8[capacity]
+//   vecs_fp8  [capacity x D]  optional e4m3 copy + per row (scale, scale^2 |codes|^2)
 //   vecs_u8   [capacity x D]  optional uint8 copy
 //   deg       [capacity]      u32 out-degree
 //   adj       [capacity x R]  u32 neighbour ids (row stride R)
@@ -68,56 +68,47 @@ __device__ __forceinline__ uint32_t bloom_pack(uint32_t x) { return (bloom_h1(x)
 // per lane group are gathered per round with all loads in flight first, so a
 // round covers G = M * 32 / T rows: 8 (FP32), 16 (BF16) or 32 (one-byte rows).
 // Dimension class DC: D <= 128 << DC.
+// widen2 / codes2 give the elements of a 16-byte chunk as pairs (element 2p in .x,
+// 2p + 1 in .y) for the packed FP32 arithmetic of sm_100 (__ffma2_rn: two FMAs
+// per instruction).
 struct StoreF32 {
     static constexpr int  kElems = 4, kLanes128 = 32, kM = 8;
     static constexpr bool kScaled = false, kInt = false;
-    __device__ __forceinline__ static void widen(const uint4& r, float, float (&o)[4]) {
-        o[0] = __uint_as_float(r.x);
-        o[1] = __uint_as_float(r.y);
-        o[2] = __uint_as_float(r.z);
-        o[3] = __uint_as_float(r.w);
+    __device__ __forceinline__ static void widen2(const uint4& r, float2 (&o)[2]) {
+        o[0] = make_float2(__uint_as_float(r.x), __uint_as_float(r.y));
+        o[1] = make_float2(__uint_as_float(r.z), __uint_as_float(r.w));
     }
 };
 struct StoreBF16 {
     static constexpr int  kElems = 8, kLanes128 = 16, kM = 8;
     static constexpr bool kScaled = false, kInt = false;
-    __device__ __forceinline__ static void widen(const uint4& r, float, float (&o)[8]) {
+    // a BF16 is the upper half of its FP32 value
+    __device__ __forceinline__ static void widen2(const uint4& r, float2 (&o)[4]) {
         const uint32_t w[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            o[2 * i]     = __uint_as_float(w[i] << 16);
-            o[2 * i + 1] = __uint_as_float(w[i] & 0xffff0000u);
-        }
+        for (int i = 0; i < 4; ++i) o[i] = make_float2(__uint_as_float(w[i] << 16), __uint_as_float(w[i] & 0xffff0000u));
     }
 };
 struct StoreFP8 {
     static constexpr int  kElems = 16, kLanes128 = 8, kM = 8;
     static constexpr bool kScaled = true, kInt = false;
-    // the 16 codes of a chunk as floats, unscaled (e4m3 -> f16 -> f32 is exact)
-    __device__ __forceinline__ static void codes(const uint4& r, float (&o)[16]) {
+    // the 16 codes of a chunk, unscaled: one e4m3x2 -> f16x2 conversion per pair,
+    // then f16 -> f32 (both exact)
+    __device__ __forceinline__ static void codes2(const uint4& r, float2 (&o)[8]) {
         const uint32_t w[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             __half2_raw lo = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[i] & 0xffffu), __NV_E4M3);
             __half2_raw hi = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[i] >> 16), __NV_E4M3);
-            float2 a = __half22float2(*reinterpret_cast<__half2*>(&lo));
-            float2 b = __half22float2(*reinterpret_cast<__half2*>(&hi));
-            o[4 * i]     = a.x;
-            o[4 * i + 1] = a.y;
-            o[4 * i + 2] = b.x;
-            o[4 * i + 3] = b.y;
+            o[2 * i]       = __half22float2(*reinterpret_cast<__half2*>(&lo));
+            o[2 * i + 1]   = __half22float2(*reinterpret_cast<__half2*>(&hi));
         }
-    }
-    __device__ __forceinline__ static void widen(const uint4& r, float s, float (&o)[16]) {
-        codes(r, o);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) o[i] *= s;
     }
 };
 struct StoreU8 {
     static constexpr int  kElems = 16, kLanes128 = 8, kM = 8;
     static constexpr bool kScaled = false, kInt = true;  // exact dp4a path for integer queries
-    __device__ __forceinline__ static void widen(const uint4& r, float, float (&o)[16]) {
+    __device__ __forceinline__ static void widen(const uint4& r, float (&o)[16]) {
         const uint32_t w[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
@@ -153,9 +144,9 @@ __device__ __forceinline__ uint4 load16(const void* base, uint64_t row_bytes, ui
 // [0, 255] (uint8 rows then use exact dp4a integer arithmetic).
 template <typename S, int DC>
 struct Query {
-    // FP32 copy of the lane's chunks (integer stores keep none: their rare
-    // non-integer fallback re-reads the row through L1)
-    float        f[S::kInt ? 1 : Layout<S, DC>::kCPL][S::kInt ? 1 : S::kElems];
+    // FP32 copy of the lane's chunks as element pairs (integer stores keep none:
+    // their rare non-integer fallback re-reads the row through L1)
+    float2       f2[S::kInt ? 1 : Layout<S, DC>::kCPL][S::kInt ? 1 : S::kElems / 2];
     uint32_t     u[Layout<S, DC>::kCPL][S::kElems / 4];
     const float* row;
     int          qq;
@@ -163,8 +154,11 @@ struct Query {
     bool         qint;
 };
 
+// center (scaled stores): the per-dimension centre the row codes are relative to;
+// the query is centred the same way, which leaves every distance unchanged.
 template <typename S, int DC>
-__device__ __forceinline__ void load_query(Query<S, DC>& q, const float* row, uint32_t D, uint32_t lane) {
+__device__ __forceinline__ void load_query(Query<S, DC>& q, const float* row, uint32_t D, uint32_t lane,
+                                           const float* center = nullptr) {
     using Ly              = Layout<S, DC>;
     const uint32_t chunks = D / S::kElems;
     const uint32_t t      = lane % Ly::kT;
@@ -179,11 +173,23 @@ __device__ __forceinline__ void load_query(Query<S, DC>& q, const float* row, ui
         for (int v = 0; v < S::kElems / 4; ++v) {
             float4 x = valid ? __ldg(reinterpret_cast<const float4*>(row + k * S::kElems) + v)
                              : make_float4(0.f, 0.f, 0.f, 0.f);
+            if constexpr (S::kScaled) {
+                if (center != nullptr && valid) {
+                    const float4 cz = __ldg(reinterpret_cast<const float4*>(center + k * S::kElems) + v);
+                    x.x -= cz.x;
+                    x.y -= cz.y;
+                    x.z -= cz.z;
+                    x.w -= cz.w;
+                }
+            }
             float  e[4] = {x.x, x.y, x.z, x.w};
+            if constexpr (!S::kInt) {
+                q.f2[c][2 * v]     = make_float2(x.x, x.y);
+                q.f2[c][2 * v + 1] = make_float2(x.z, x.w);
+            }
             uint32_t pk = 0;
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                if constexpr (!S::kInt) q.f[c][4 * v + i] = e[i];
                 if constexpr (S::kScaled) qn = fmaf(e[i], e[i], qn);
                 bool good = e[i] >= 0.f && e[i] <= 255.f && rintf(e[i]) == e[i];
                 ok &= good;
@@ -254,7 +260,7 @@ __device__ __forceinline__ bool round_writer(uint32_t lane) {
 // a partial round): no loads and no arithmetic.  (The same branch around the
 // float stores' loads costs more than it saves.)
 template <typename S, int DC, typename IdFn>
-__device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* base, const float* scale,
+__device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* base, const float2* scale,
                                             IdFn ids, int cnt, uint32_t D, uint32_t lane) {
     using Ly                 = Layout<S, DC>;
     constexpr int  M         = Ly::kM;
@@ -263,13 +269,13 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
     const uint32_t t         = lane % Ly::kT;
     const uint32_t g         = lane / Ly::kT;
     uint4          x[M][Ly::kCPL];
-    float          sc[M];
+    float2         sc[M];  // scaled rows: (scale, scale^2 |codes|^2)
 #pragma unroll
     for (int m = 0; m < M; ++m) {
         if (S::kInt && m * Ly::kP >= cnt) {
 #pragma unroll
             for (int c = 0; c < Ly::kCPL; ++c) x[m][c] = make_uint4(0u, 0u, 0u, 0u);
-            sc[m] = 0.f;
+            sc[m] = make_float2(0.f, 0.f);
             continue;
         }
         const int r     = m * Ly::kP + (int)g;
@@ -280,8 +286,8 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
             uint32_t k = t + (uint32_t)Ly::kT * c;
             x[m][c]    = (valid && k < chunks) ? load16(base, row_bytes, id, k) : make_uint4(0u, 0u, 0u, 0u);
         }
-        if constexpr (S::kScaled) sc[m] = valid ? __ldg(scale + id) : 0.f;
-        else sc[m] = 1.f;
+        if constexpr (S::kScaled) sc[m] = valid ? __ldg(scale + id) : make_float2(0.f, 0.f);
+        else sc[m] = make_float2(1.f, 0.f);
     }
     if constexpr (S::kInt) {
         if (q.qint) {
@@ -308,57 +314,81 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
     }
     if constexpr (S::kScaled) {
         // sum (q - s c)^2 = |q|^2 - 2 s (q . c) + s^2 |c|^2: the codes are widened
-        // unscaled, and each row's scale is applied once, not once per element
+        // unscaled, q . c runs on element pairs, each row's scale is applied once,
+        // and s^2 |c|^2 is stored beside the scale (added by one lane per group)
+        float2 qc[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) qc[m] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+#pragma unroll
+            for (int c = 0; c < Ly::kCPL; ++c) {
+                float2 e[S::kElems / 2];
+                S::codes2(x[m][c], e);
+#pragma unroll
+                for (int p = 0; p < S::kElems / 2; ++p) qc[m] = __ffma2_rn(q.f2[c][p], e[p], qc[m]);
+            }
+        }
         float v[M];
 #pragma unroll
         for (int m = 0; m < M; ++m) {
-            float qc = 0.f, cc = 0.f;
-#pragma unroll
-            for (int c = 0; c < Ly::kCPL; ++c) {
-                float e[S::kElems];
-                S::codes(x[m][c], e);
-#pragma unroll
-                for (int i = 0; i < S::kElems; ++i) {
-                    qc = fmaf(q.f[c][i], e[i], qc);
-                    cc = fmaf(e[i], e[i], cc);
-                }
-            }
-            v[m] = fmaf(sc[m] * sc[m], cc, fmaf(-2.f * sc[m], qc, q.qn));
+            v[m] = fmaf(-2.f * sc[m].x, qc[m].x + qc[m].y, q.qn);
+            if (t == 0u) v[m] += sc[m].y;
         }
         // rounding can leave a tiny negative for a row equal to the query
         return fmaxf(group_reduce<M, Ly::kT, float>(v, lane), 0.f);
-    }
-    float v[M];
+    } else if constexpr (!S::kInt) {
+        float v[M];
+        // (x - q)^2 on element pairs: x - q = fma(q, -1, x), then fma(d, d, acc)
+        const float2 neg1 = make_float2(-1.f, -1.f);
+        float2       acc[M];
 #pragma unroll
-    for (int m = 0; m < M; ++m) v[m] = 0.f;
+        for (int m = 0; m < M; ++m) acc[m] = make_float2(0.f, 0.f);
 #pragma unroll
-    for (int c = 0; c < Ly::kCPL; ++c) {
-        float e[M][S::kElems];
+        for (int c = 0; c < Ly::kCPL; ++c) {
 #pragma unroll
-        for (int m = 0; m < M; ++m) S::widen(x[m][c], sc[m], e[m]);
-        float qf[S::kElems];
-        if constexpr (S::kInt) {
+            for (int m = 0; m < M; ++m) {
+                float2 e[S::kElems / 2];
+                S::widen2(x[m][c], e);
+#pragma unroll
+                for (int p = 0; p < S::kElems / 2; ++p) {
+                    const float2 d = __ffma2_rn(q.f2[c][p], neg1, e[p]);
+                    acc[m]         = __ffma2_rn(d, d, acc[m]);
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < M; ++m) v[m] = acc[m].x + acc[m].y;
+        return group_reduce<M, Ly::kT, float>(v, lane);
+    } else {
+        // integer rows with a query that is not (rare): FP32 from the row bytes and
+        // the query re-read through L1
+        float v[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) v[m] = 0.f;
+#pragma unroll
+        for (int c = 0; c < Ly::kCPL; ++c) {
             const uint32_t k = t + (uint32_t)Ly::kT * c;
+            float          qf[S::kElems];
 #pragma unroll
             for (int v4 = 0; v4 < S::kElems / 4; ++v4) {
                 float4 z = k < chunks ? __ldg(reinterpret_cast<const float4*>(q.row + k * S::kElems) + v4)
                                       : make_float4(0.f, 0.f, 0.f, 0.f);
-                qf[4 * v4] = z.x;
+                qf[4 * v4]     = z.x;
                 qf[4 * v4 + 1] = z.y;
                 qf[4 * v4 + 2] = z.z;
                 qf[4 * v4 + 3] = z.w;
             }
-        } else {
 #pragma unroll
-            for (int i = 0; i < S::kElems; ++i) qf[i] = q.f[c][i];
+            for (int m = 0; m < M; ++m) {
+                float e[S::kElems];
+                S::widen(x[m][c], e);
+#pragma unroll
+                for (int i = 0; i < S::kElems; ++i) v[m] = sqdiff(qf[i], e[i], v[m]);
+            }
         }
-#pragma unroll
-        for (int i = 0; i < S::kElems; ++i) {
-#pragma unroll
-            for (int m = 0; m < M; ++m) v[m] = sqdiff(qf[i], e[m][i], v[m]);
-        }
+        return group_reduce<M, Ly::kT, float>(v, lane);
     }
-    return group_reduce<M, Ly::kT, float>(v, lane);
 }
 
 // ---------------------------------------------------------------- launches

@@ -62,8 +62,32 @@ cudaError_t launch_hash_rows(const uint32_t* adj, uint32_t* adj_h, uint64_t n, u
 
 // FP32 rows -> traversal copies.  FP8: scale = amax / 448 per row (e4m3 max
 // finite 448), codes = satfinite(x / scale).  U8: round to nearest, clamp.
-__global__ void convert_kernel(const float* src, void* dst, float* scale, uint64_t rows, uint32_t D,
-                               int store, uint32_t* inexact) {
+// One row's e4m3 codes (one warp): the row is centred (row - center), s = amax / 448
+// of the centred row, codes = centred row / s rounded to e4m3 (saturating), and
+// beside s the squared norm of the decoded codes times s^2, which the traversal
+// distance adds once per row.  Centring uses the format's sign bit for rows that
+// are all non-negative, halving the scale and so the rounding error.
+__device__ void fp8_row(const float* src, uint8_t* d, float2* scale, const float* center, uint32_t D,
+                        uint32_t lane) {
+    float amax = 0.f;
+    for (uint32_t i = lane; i < D; i += 32) amax = fmaxf(amax, fabsf(src[i] - center[i]));
+    for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    const float sc  = amax > 0.f ? amax / 448.f : 1.f;
+    const float inv = 1.f / sc;
+    float       cc  = 0.f;
+    for (uint32_t i = lane; i < D; i += 32) {
+        const __nv_fp8_storage_t c = __nv_cvt_float_to_fp8((src[i] - center[i]) * inv, __NV_SATFINITE, __NV_E4M3);
+        d[i]                       = (uint8_t)c;
+        const __half_raw h         = __nv_cvt_fp8_to_halfraw(c, __NV_E4M3);
+        const float      v         = __half2float(*reinterpret_cast<const __half*>(&h));
+        cc                         = fmaf(v, v, cc);
+    }
+    for (int o = 16; o; o >>= 1) cc += __shfl_xor_sync(0xffffffffu, cc, o);
+    if (lane == 0) *scale = make_float2(sc, sc * sc * cc);
+}
+
+__global__ void convert_kernel(const float* src, void* dst, float2* scale, const float* center, uint64_t rows,
+                               uint32_t D, int store, uint32_t* inexact) {
     uint64_t r    = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
     uint32_t lane = threadIdx.x & 31u;
     if (r >= rows) return;
@@ -72,15 +96,7 @@ __global__ void convert_kernel(const float* src, void* dst, float* scale, uint64
         __nv_bfloat16* d = static_cast<__nv_bfloat16*>(dst) + r * D;
         for (uint32_t i = lane; i < D; i += 32) d[i] = __float2bfloat16_rn(s[i]);
     } else if (store == 2) {
-        float amax = 0.f;
-        for (uint32_t i = lane; i < D; i += 32) amax = fmaxf(amax, fabsf(s[i]));
-        for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-        float sc  = amax > 0.f ? amax / 448.f : 1.f;
-        float inv = 1.f / sc;
-        uint8_t* d = static_cast<uint8_t*>(dst) + r * D;
-        for (uint32_t i = lane; i < D; i += 32)
-            d[i] = (uint8_t)__nv_cvt_float_to_fp8(s[i] * inv, __NV_SATFINITE, __NV_E4M3);
-        if (lane == 0) scale[r] = sc;
+        fp8_row(s, static_cast<uint8_t*>(dst) + r * D, scale + r, center, D, lane);
     } else if (store == 3) {
         uint8_t* d   = static_cast<uint8_t*>(dst) + r * D;
         bool     off = false;
@@ -94,17 +110,17 @@ __global__ void convert_kernel(const float* src, void* dst, float* scale, uint64
     }
 }
 
-cudaError_t launch_convert(const float* src, void* dst, float* scale, uint64_t rows, uint32_t D,
-                           int store, uint32_t* inexact, cudaStream_t st) {
+cudaError_t launch_convert(const float* src, void* dst, float2* scale, const float* center, uint64_t rows,
+                           uint32_t D, int store, uint32_t* inexact, cudaStream_t st) {
     if (rows == 0) return cudaSuccess;
-    convert_kernel<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(src, dst, scale, rows, D, store, inexact);
+    convert_kernel<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(src, dst, scale, center, rows, D, store, inexact);
     return cudaGetLastError();
 }
 
 // Same conversion for rows scattered over an id list (inserts into reused ids):
 // one warp per listed row, the row's traversal copy rewritten from its FP32 row.
 __global__ void convert_ids_kernel(const float* vecs, const uint32_t* ids, uint64_t n, void* dst,
-                                   float* scale, uint32_t D, int store, uint32_t* inexact) {
+                                   float2* scale, const float* center, uint32_t D, int store, uint32_t* inexact) {
     uint64_t i    = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
     uint32_t lane = threadIdx.x & 31u;
     if (i >= n) return;
@@ -114,15 +130,7 @@ __global__ void convert_ids_kernel(const float* vecs, const uint32_t* ids, uint6
         __nv_bfloat16* d = static_cast<__nv_bfloat16*>(dst) + r * D;
         for (uint32_t k = lane; k < D; k += 32) d[k] = __float2bfloat16_rn(s[k]);
     } else if (store == 2) {
-        float amax = 0.f;
-        for (uint32_t k = lane; k < D; k += 32) amax = fmaxf(amax, fabsf(s[k]));
-        for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-        float    sc  = amax > 0.f ? amax / 448.f : 1.f;
-        float    inv = 1.f / sc;
-        uint8_t* d   = static_cast<uint8_t*>(dst) + r * D;
-        for (uint32_t k = lane; k < D; k += 32)
-            d[k] = (uint8_t)__nv_cvt_float_to_fp8(s[k] * inv, __NV_SATFINITE, __NV_E4M3);
-        if (lane == 0) scale[r] = sc;
+        fp8_row(s, static_cast<uint8_t*>(dst) + r * D, scale + r, center, D, lane);
     } else if (store == 3) {
         uint8_t* d   = static_cast<uint8_t*>(dst) + r * D;
         bool     off = false;
@@ -134,10 +142,12 @@ __global__ void convert_ids_kernel(const float* vecs, const uint32_t* ids, uint6
         if (__any_sync(0xffffffffu, off) && lane == 0) atomicOr(inexact, 1u);
     }
 }
-cudaError_t launch_convert_ids(const float* vecs, const uint32_t* ids, uint64_t n, void* dst, float* scale,
+cudaError_t launch_convert_ids(const float* vecs, const uint32_t* ids, uint64_t n, void* dst, float2* scale,
+                               const float* center,
                                uint32_t D, int store, uint32_t* inexact, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
-    convert_ids_kernel<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(vecs, ids, n, dst, scale, D, store, inexact);
+    convert_ids_kernel<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(vecs, ids, n, dst, scale, center, D, store,
+                                                                inexact);
     return cudaGetLastError();
 }
 
@@ -228,16 +238,13 @@ unsigned long long* medoid_best(void* ws, uint32_t D) {
     return reinterpret_cast<unsigned long long*>(static_cast<char*>(ws) + align16(sizeof(double) * D) +
                                                  align16(sizeof(uint32_t) * D));
 }
-cudaError_t launch_medoid(const float* vecs, uint64_t n, uint32_t D, void* ws, uint32_t* d_out, cudaStream_t st) {
-    if (n == 0 || D == 0) return cudaErrorInvalidValue;
-    auto*               sum   = static_cast<unsigned long long*>(ws);
-    auto*               bound = reinterpret_cast<uint32_t*>(static_cast<char*>(ws) + align16(sizeof(double) * D));
-    unsigned long long* best  = medoid_best(ws, D);
-    int lg = 1;  // ceil(log2(n)), at least 1
+static cudaError_t launch_col_means_f64(const float* vecs, uint64_t n, uint32_t D, void* ws, cudaStream_t st) {
+    auto* sum   = static_cast<unsigned long long*>(ws);
+    auto* bound = reinterpret_cast<uint32_t*>(static_cast<char*>(ws) + align16(sizeof(double) * D));
+    int   lg    = 1;  // ceil(log2(n)), at least 1
     while (lg < 63 && (1ull << lg) < n) ++lg;
     const int   B = 62 - lg;
     cudaError_t e = cudaMemsetAsync(ws, 0, align16(sizeof(double) * D) + align16(sizeof(uint32_t) * D), st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(best, 0xff, 2 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     const dim3 g((unsigned)((n + 1023) / 1024), (D + 127) / 128);
     col_bound_kernel<<<g, 128, 0, st>>>(vecs, n, D, bound);
@@ -245,8 +252,29 @@ cudaError_t launch_medoid(const float* vecs, uint64_t n, uint32_t D, void* ws, u
     col_sum_kernel<<<g, 128, 0, st>>>(vecs, n, D, bound, B, sum);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     col_mean_kernel<<<(D + 127) / 128, 128, 0, st>>>(n, D, bound, B, sum);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    const double* mean = reinterpret_cast<const double*>(sum);
+    return cudaGetLastError();
+}
+
+__global__ void f64_to_f32_kernel(const double* in, uint32_t n, float* out) {
+    const uint32_t i = threadIdx.x + blockIdx.x * blockDim.x;
+    if (i < n) out[i] = (float)in[i];
+}
+
+cudaError_t launch_col_mean(const float* vecs, uint64_t n, uint32_t D, void* ws, float* mean, cudaStream_t st) {
+    if (n == 0 || D == 0) return cudaErrorInvalidValue;
+    cudaError_t e = launch_col_means_f64(vecs, n, D, ws, st);
+    if (e != cudaSuccess) return e;
+    f64_to_f32_kernel<<<(D + 127) / 128, 128, 0, st>>>(static_cast<const double*>(ws), D, mean);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_medoid(const float* vecs, uint64_t n, uint32_t D, void* ws, uint32_t* d_out, cudaStream_t st) {
+    if (n == 0 || D == 0) return cudaErrorInvalidValue;
+    unsigned long long* best = medoid_best(ws, D);
+    cudaError_t         e    = launch_col_means_f64(vecs, n, D, ws, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(best, 0xff, 2 * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    const double* mean = static_cast<const double*>(ws);
     for (int pass = 0; pass < 2; ++pass) {
         medoid_dist_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(vecs, n, D, mean, best, pass);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -206,7 +206,8 @@ struct vann_index {
 
     float*    vecs  = nullptr;
     void*     store[4] = {nullptr, nullptr, nullptr, nullptr};
-    float*    fp8_scale = nullptr;
+    float2*   fp8_scale = nullptr;  // per row (scale, scale^2 |codes|^2)
+    float*    fp8_center = nullptr; // per dimension: the FP8 codes encode row - center
     uint32_t* deg  = nullptr;
     uint32_t* adj  = nullptr;
     uint32_t* adj_h = nullptr;  // packed filter slots beside every adjacency entry
@@ -247,6 +248,7 @@ struct vann_index {
         cudaFree(vecs);
         for (void* s : store) cudaFree(s);
         cudaFree(fp8_scale);
+        cudaFree(fp8_center);
         cudaFree(deg);
         cudaFree(adj);
         cudaFree(adj_h);
@@ -322,16 +324,21 @@ struct vann_index {
     }
 
     // rows [first, first + rows) -> traversal copies; rows from 0 replace every
-    // row, so the uint8 exactness flag starts over
+    // row, so the uint8 exactness flag starts over and the FP8 centre (the rows'
+    // column means, fixed until the rows are replaced again) is recomputed
     void convert_rows(uint64_t first, uint64_t rows, cudaStream_t st) {
         u8_state = -1;
         if (first == 0) VCHECK(cudaMemsetAsync(u8_inexact(), 0, sizeof(uint32_t), st));
+        if (first == 0 && store[2] && rows > 0) {
+            medoid_ws.ensure(vann::medoid_ws_bytes(p.dim));
+            VCHECK(vann::launch_col_mean(vecs, rows, p.dim, medoid_ws.p, fp8_center, st));
+        }
         for (int s = 1; s < 4; ++s) {
             if (!store[s]) continue;
             size_t esz = s == 1 ? 2 : 1;
             void*  dst = static_cast<char*>(store[s]) + first * p.dim * esz;
             VCHECK(vann::launch_convert(vecs + first * p.dim, dst, s == 2 ? fp8_scale + first : nullptr,
-                                        rows, p.dim, s, u8_inexact(), st));
+                                        s == 2 ? fp8_center : nullptr, rows, p.dim, s, u8_inexact(), st));
         }
     }
 
@@ -651,7 +658,8 @@ vann_status vann_create(const vann_params* params, vann_index** out) {
             if (p.stores & (1u << VANN_STORE_BF16)) h->alloc(&h->store[1], 2ull * C * p.dim);
             if (p.stores & (1u << VANN_STORE_FP8)) {
                 h->alloc(&h->store[2], 1ull * C * p.dim);
-                h->alloc((void**)&h->fp8_scale, sizeof(float) * C);
+                h->alloc((void**)&h->fp8_scale, sizeof(float2) * C);
+                h->alloc((void**)&h->fp8_center, sizeof(float) * p.dim);
             }
             if (p.stores & (1u << VANN_STORE_U8)) h->alloc(&h->store[3], 1ull * C * p.dim);
             h->store[0] = h->vecs;
@@ -988,6 +996,7 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
         a.beam  = vann_index::beam_of(*sp);
         a.store = h->store[sp->store];
         a.scale = h->fp8_scale;
+        a.center = sp->store == VANN_STORE_FP8 ? h->fp8_center : nullptr;
         a.vecs_f32 = h->vecs;
         a.deg = h->deg;
         a.adj = h->adj;
@@ -1192,7 +1201,8 @@ vann_status vann_insert(vann_index* h, const float* d_vecs, uint64_t n, uint32_t
             for (int s = 1; s < 4; ++s)  // reused ids are scattered: convert by id list
                 if (h->store[s])
                     VCHECK(vann::launch_convert_ids(h->vecs, h->nodes.as<uint32_t>(), n, h->store[s],
-                                                    s == 2 ? h->fp8_scale : nullptr, D, s, h->u8_inexact(), st));
+                                                    s == 2 ? h->fp8_scale : nullptr, s == 2 ? h->fp8_center : nullptr,
+                                                    D, s, h->u8_inexact(), st));
         }
         h->size += n - reuse;
         const bool parity = (h->p.flags & VANN_QUIRK_SKIP_BATCH_INDEX) != 0;

@@ -13,7 +13,8 @@ void set_last_error(const char* msg);
 
 struct SearchArgs {
     const void*     store;     // traversal copy (F32 / BF16 / FP8 / U8 rows)
-    const float*    scale;     // per-row scale of the FP8 copy
+    const float2*   scale;     // FP8 copy: per row (scale, scale^2 * |codes|^2)
+    const float*    center;    // FP8 copy: per-dimension centre the codes are relative to
     const float*    vecs_f32;  // exact rows (rerank)
     const uint32_t* deg;
     const uint32_t* adj;
@@ -122,10 +123,14 @@ cudaError_t launch_random_graph(uint32_t* deg, uint32_t* adj, uint32_t* adj_h, u
 cudaError_t launch_hash_rows(const uint32_t* adj, uint32_t* adj_h, uint64_t n, uint32_t R,
                              cudaStream_t st);
 // inexact: set non-zero when a uint8 code is not exactly its FP32 value
-cudaError_t launch_convert(const float* src, void* dst, float* scale, uint64_t rows, uint32_t D,
-                           int store, uint32_t* inexact, cudaStream_t st);
-cudaError_t launch_convert_ids(const float* vecs, const uint32_t* ids, uint64_t n, void* dst, float* scale,
-                               uint32_t D, int store, uint32_t* inexact, cudaStream_t st);
+// FP8 only: the codes encode row - center[] with scale[row] = (s, s^2 * |codes|^2),
+// s = amax / 448 of the centred row
+cudaError_t launch_convert(const float* src, void* dst, float2* scale, const float* center, uint64_t rows,
+                           uint32_t D, int store, uint32_t* inexact, cudaStream_t st);
+cudaError_t launch_convert_ids(const float* vecs, const uint32_t* ids, uint64_t n, void* dst, float2* scale,
+                               const float* center, uint32_t D, int store, uint32_t* inexact, cudaStream_t st);
+// FP32 column means of rows 0 .. n-1 (the medoid's exact column sums); ws: medoid_ws_bytes(D)
+cudaError_t launch_col_mean(const float* vecs, uint64_t n, uint32_t D, void* ws, float* mean, cudaStream_t st);
 cudaError_t launch_iota(uint32_t* out, uint64_t n, uint32_t first, cudaStream_t st);
 cudaError_t launch_set_bits(uint32_t* bits, const uint32_t* ids, uint64_t n, uint64_t limit,
                             cudaStream_t st);

@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
         const uint32_t kq = a.kq != nullptr ? min(__ldg(a.kq + q), a.k) : a.k;
 
         Query<S, DC> qv;
-        load_query<S, DC>(qv, a.queries + (uint64_t)q * a.D, a.D, lane);
+        load_query<S, DC>(qv, a.queries + (uint64_t)q * a.D, a.D, lane, a.center);
         for (uint32_t w = lane; w < kBloomWords; w += 32) bloom[w] = 0u;
 
         uint32_t skip = kNone;

@@ -25,14 +25,79 @@ constexpr uint64_t kSentinel = ~0ull;
 
 struct RegLayout {
     uint32_t maxr;   // candidate slots (>= 64 so that the rerank ids fit too)
-    uint32_t bytes;  // per warp: bloom filter + candidate ids/distances
+    uint32_t bytes;  // per warp: bloom filter + candidate ids/distances + 64 merge payloads
     __host__ __device__ static RegLayout make(uint32_t slots) {
         RegLayout l;
         l.maxr  = slots < 64u ? 64u : slots;
-        l.bytes = 5008u + 8u * l.maxr;
+        l.bytes = 5008u + 8u * l.maxr + 256u;
         return l;
     }
 };
+
+// Kept candidates up to this count are merged by rank (below); more go through
+// the bitonic sort and merge network.
+constexpr uint32_t kRankMergeMax = 12;
+
+// Merge of kc <= 32 kept candidates (keys (distance bits << 32 | id) in cand[0 .. kc),
+// unsorted) into the register worklist by counting ranks: candidate j goes to
+// (worklist entries at or below its distance) + (candidates before it in (distance,
+// id) order); worklist entry e moves down by the candidates strictly closer.  That is
+// the order the sort + merge network gives (equal distances: older entries first,
+// new ones by id), in about a dozen instructions per candidate instead of two
+// networks of shuffles.  Positions at or beyond L fall off; the new entries take
+// insertion sequences seq + rank.  skey / spay: 64 staging slots in shared memory
+// (skey may alias cand: it is written after every lane has read cand).
+template <int LREG>
+__device__ __forceinline__ void rank_merge(uint64_t (&wk)[LREG], uint32_t (&wp)[LREG], const uint64_t* cand,
+                                           uint32_t kc, uint32_t seq, uint32_t& n, uint32_t L, uint64_t* skey,
+                                           uint32_t* spay, uint32_t lane) {
+    const uint64_t cj    = lane < kc ? cand[lane] : kSentinel;
+    uint32_t       crank = 0, cpos = 0;
+    uint32_t       wsh[LREG];
+    uint32_t       wd[LREG];
+#pragma unroll
+    for (int r = 0; r < LREG; ++r) {
+        wsh[r] = 0u;
+        wd[r]  = (uint32_t)(wk[r] >> 32);  // sentinels: 0xFFFFFFFF, above every distance
+    }
+    for (uint32_t k = 0; k < kc; ++k) {
+        const uint64_t ck = cand[k];
+        const uint32_t cd = (uint32_t)(ck >> 32);
+        crank += (ck < cj || (ck == cj && k < lane)) ? 1u : 0u;
+        uint32_t before = 0;
+#pragma unroll
+        for (int r = 0; r < LREG; ++r) {
+            wsh[r] += cd < wd[r] ? 1u : 0u;
+            before += __popc(__ballot_sync(0xffffffffu, wd[r] <= cd));
+        }
+        if (lane == k) cpos = before;
+    }
+    __syncwarp();  // every lane has read cand: skey may overwrite it
+#pragma unroll
+    for (int r = 0; r < LREG; ++r) {
+        const uint32_t p = (uint32_t)r * 32u + lane + wsh[r];
+        if (wk[r] != kSentinel && p < L) {
+            skey[p] = wk[r];
+            spay[p] = wp[r];
+        }
+    }
+    if (lane < kc) {
+        const uint32_t p = cpos + crank;
+        if (p < L) {
+            skey[p] = (cj & 0xffffffff00000000ull) | (uint64_t)(seq + crank);
+            spay[p] = (uint32_t)cj;
+        }
+    }
+    __syncwarp();
+    n = min(n + kc, L);
+#pragma unroll
+    for (int r = 0; r < LREG; ++r) {
+        const uint32_t e = (uint32_t)r * 32u + lane;
+        wk[r]            = e < n ? skey[e] : kSentinel;
+        wp[r]            = e < n ? spay[e] : 0u;
+    }
+    __syncwarp();
+}
 
 // Lower half of the union of two ascending sequences of N = 32 * LREG keys,
 // sorted ascending in place in (wk, wp).  Keys are unique except sentinels.
@@ -89,6 +154,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
     uint32_t*       nb_id = reinterpret_cast<uint32_t*>(base + 5008);
     float*          nb_d  = reinterpret_cast<float*>(base + 5008 + 4 * lay.maxr);
     uint64_t*       nb_key = reinterpret_cast<uint64_t*>(nb_id);  // after ids/dists are read
+    uint32_t*       m_pay = reinterpret_cast<uint32_t*>(base + 5008 + 8 * lay.maxr);  // rank-merge payloads
     uint64_t*       rkeys = reinterpret_cast<uint64_t*>(base);     // rerank keys, after the search
     const uint32_t  R     = a.R;
 
@@ -104,7 +170,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
         const uint32_t kq = a.kq != nullptr ? min(__ldg(a.kq + q), a.k) : a.k;
 
         Query<S, DC> qv;
-        load_query<S, DC>(qv, a.queries + (uint64_t)q * a.D, a.D, lane);
+        load_query<S, DC>(qv, a.queries + (uint64_t)q * a.D, a.D, lane, a.center);
         for (uint32_t w = lane; w < kBloomWords; w += 32) bloom[w] = 0u;
 
         uint32_t skip = kNone;
@@ -244,6 +310,11 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
             }
             __syncwarp();
 
+            if (BEAM == 1 && kc > 0u && kc <= kRankMergeMax) {
+                rank_merge<LREG>(wk, wp, nb_key, kc, seq, n, L, nb_key, m_pay, lane);
+                seq += kc;
+                kc = 0u;  // merged
+            }
             // at most 64 kept candidates per batch (one batch unless BEAM = 2)
             for (uint32_t b0 = 0; b0 < kc; b0 += 64u) {
                 const uint32_t  bc = min(64u, kc - b0);
