@@ -133,10 +133,23 @@ struct Layout {
     static constexpr int  kP   = 32 / kT;              // rows per warp load
     static constexpr int  kM   = kNarrow ? 4 : S::kM;  // rows per lane per round
     static constexpr int  kG   = kM * kP;              // rows per gather round
+    // chunk c of lane group member t: integer rows of 128 bytes give each lane two
+    // adjacent chunks (32 contiguous bytes, one 256-bit load); the others interleave
+    __device__ __forceinline__ static uint32_t chunk(uint32_t t, int c) {
+        return kNarrow ? t * (uint32_t)kCPL + (uint32_t)c : t + (uint32_t)kT * (uint32_t)c;
+    }
 };
 
 __device__ __forceinline__ uint4 load16(const void* base, uint64_t row_bytes, uint64_t row, uint32_t k) {
     return __ldg(reinterpret_cast<const uint4*>(static_cast<const unsigned char*>(base) + row * row_bytes) + k);
+}
+// chunks k and k + 1 of a row (32 bytes, 32-byte aligned) in one 256-bit load
+__device__ __forceinline__ void load32(const void* base, uint64_t row_bytes, uint64_t row, uint32_t k, uint4& a,
+                                       uint4& b) {
+    const unsigned char* p = static_cast<const unsigned char*>(base) + row * row_bytes + 16ull * k;
+    asm("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+        : "l"(p));
 }
 
 // Register-resident query in the lane layout of store S: the lane's chunks in
@@ -167,7 +180,7 @@ __device__ __forceinline__ void load_query(Query<S, DC>& q, const float* row, ui
     float          qn     = 0.f;
 #pragma unroll
     for (int c = 0; c < Ly::kCPL; ++c) {
-        uint32_t k     = t + (uint32_t)Ly::kT * c;
+        uint32_t k     = Ly::chunk(t, c);
         bool     valid = k < chunks;
 #pragma unroll
         for (int v = 0; v < S::kElems / 4; ++v) {
@@ -281,10 +294,23 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
         const int r     = m * Ly::kP + (int)g;
         const bool valid = r < cnt;
         uint32_t   id    = valid ? ids(r) : 0u;
+        if constexpr (Ly::kNarrow) {
+            // the lane's two chunks are adjacent: one 256-bit load when both lie in
+            // the row and rows are 32-byte aligned (row bytes a multiple of 32)
+            const uint32_t k0 = Ly::chunk(t, 0);
+            if (valid && k0 + 1u < chunks && (row_bytes & 31u) == 0u) {
+                load32(base, row_bytes, id, k0, x[m][0], x[m][1]);
+            } else {
+                x[m][0] = (valid && k0 < chunks) ? load16(base, row_bytes, id, k0) : make_uint4(0u, 0u, 0u, 0u);
+                x[m][1] = (valid && k0 + 1u < chunks) ? load16(base, row_bytes, id, k0 + 1u)
+                                                      : make_uint4(0u, 0u, 0u, 0u);
+            }
+        } else {
 #pragma unroll
-        for (int c = 0; c < Ly::kCPL; ++c) {
-            uint32_t k = t + (uint32_t)Ly::kT * c;
-            x[m][c]    = (valid && k < chunks) ? load16(base, row_bytes, id, k) : make_uint4(0u, 0u, 0u, 0u);
+            for (int c = 0; c < Ly::kCPL; ++c) {
+                uint32_t k = Ly::chunk(t, c);
+                x[m][c]    = (valid && k < chunks) ? load16(base, row_bytes, id, k) : make_uint4(0u, 0u, 0u, 0u);
+            }
         }
         if constexpr (S::kScaled) sc[m] = valid ? __ldg(scale + id) : make_float2(0.f, 0.f);
         else sc[m] = make_float2(1.f, 0.f);
@@ -368,7 +394,7 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
         for (int m = 0; m < M; ++m) v[m] = 0.f;
 #pragma unroll
         for (int c = 0; c < Ly::kCPL; ++c) {
-            const uint32_t k = t + (uint32_t)Ly::kT * c;
+            const uint32_t k = Ly::chunk(t, c);
             float          qf[S::kElems];
 #pragma unroll
             for (int v4 = 0; v4 < S::kElems / 4; ++v4) {

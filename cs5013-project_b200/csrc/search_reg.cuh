@@ -36,7 +36,7 @@ struct RegLayout {
 
 // Kept candidates up to this count are merged by rank (below); more go through
 // the bitonic sort and merge network.
-constexpr uint32_t kRankMergeMax = 12;
+constexpr uint32_t kRankMergeMax = 24;
 
 // Merge of kc <= 32 kept candidates (keys (distance bits << 32 | id) in cand[0 .. kc),
 // unsorted) into the register worklist by counting ranks: candidate j goes to
