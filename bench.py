@@ -67,10 +67,10 @@ def parse():
     ap.add_argument("--only", default=None,
                     help="FORM@L (e.g. u8@32): sweep and time that one form at that L only, no autotune "
                          "(a profiler capture of exactly one kernel instantiation)")
-    ap.add_argument("--config", default="search", choices=["search", "churn", "precision", "serve", "build"],
+    ap.add_argument("--config", default="search", choices=["search", "churn", "precision", "serve", "build", "pq"],
                     help="search: the headline line; churn / precision / serve: FreshVamana churn on 1M, "
                          "reduced precision on 5M x 96, serving on 10M; build: index build and insert "
-                         "throughput (each its own JSON line)")
+                         "throughput; pq: product-quantized traversal + rerank (each its own JSON line)")
     ap.add_argument("--rounds", type=int, default=20)
     ap.add_argument("--rate", type=float, default=50_000.0, help="serve: offered requests/s")
     ap.add_argument("--duration", type=float, default=5.0, help="serve: seconds of arrivals")
@@ -1023,6 +1023,63 @@ def main_serve():
     return 0
 
 
+def main_pq():
+    """Product-quantized traversal (one byte per 8 dimensions, 256 centroids per subspace,
+    per-query distance tables) with the exact FP32 rerank, on --n x 128 rows of two
+    recipes: the benchmark's (1,000 clusters, sigma 20) and wide clusters (200 centres,
+    sigma 60).  Per recipe: recall@10 and QPS over the L sweep, the traversal distance
+    error, the uint8 form beside it, and the codes' bytes per row."""
+    args = parse()
+    import torch
+
+    import vann
+    from vann import workload
+
+    dev = torch.device("cuda", 0)
+    n, nq = args.n, args.nq
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    out = (torch.empty((nq, K), dtype=torch.int32, device=dev), torch.empty((nq, K), dtype=torch.float32, device=dev))
+    recipes = {}
+    for name, clusters, sigma in (("clusters1000_sigma20", 1000, 20.0), ("clusters200_sigma60", 200, 60.0)):
+        base_d = torch.from_numpy(workload.mixture(n, DIM, clusters, seed=1, sigma=sigma)).to(dev)
+        q_d = torch.from_numpy(workload.mixture(nq, DIM, clusters, seed=2, sigma=sigma)).to(dev)
+        idx = vann.Index(DIM, R, L_BUILD, ALPHA, capacity=n, stores=("f32", "u8", "pq"))
+        torch.cuda.synchronize()
+        t0 = time.time()
+        idx.build(base_d, batch=BATCH, seed=2024)
+        torch.cuda.synchronize()
+        build_s = time.time() - t0
+        gt = ground_truth(torch, base_d, q_d, K)
+        rows = {}
+        for store, rr in (("pq", True), ("u8", False)):
+            for L in L_SWEEP:
+                ids, d = idx.search(q_d, k=K, L=L, store=store, rerank=rr)
+                rec = recall(torch, ids, gt)
+                idx.autotune(q_d, k=K, L=L, store=store, rerank=rr)
+                t = time_steps(torch, lambda s=store, rr=rr, L=L: idx.search(q_d, k=K, L=L, store=s, rerank=rr,
+                                                                             out=out), args.steps, args.warmup, flush)
+                ent = {"L": L, "recall@10": round(rec, 4), "qps": round(nq / (statistics.mean(t) / 1e3), 1)}
+                if store == "pq":
+                    ids2, d2 = idx.search(q_d, k=K, L=L, store="pq")
+                    x = base_d[ids2.clamp(min=0).long()].double()
+                    ex = ((x - q_d.double()[:, None, :]) ** 2).sum(-1)
+                    ent["traversal_mean_rel_err"] = round(float(((d2.double() - ex).abs() / ex).mean()), 4)
+                rows.setdefault(f"{store}{'+rerank' if rr else ''}", []).append(ent)
+                if rec >= 0.995 or (store == "u8" and rec >= TARGET):
+                    break
+        recipes[name] = {"build_s": round(build_s, 2), "forms": rows}
+        del idx, base_d, q_d
+        torch.cuda.empty_cache()
+    line = {"metric": "PQ-compressed traversal + exact rerank: recall@10 and QPS against L",
+            "config": {"workload": f"{n}x{DIM} integer-valued f32 mixtures; {nq} queries; R={R} L={L_BUILD} "
+                                   f"alpha={ALPHA}; k={K}; L2 flushed before every step",
+                       "codes": f"{DIM // 8} bytes per row (8 dims per byte code, 256 centroids per subspace) "
+                                f"vs {DIM} for uint8"},
+            "data": "synthetic (seeded clipped Gaussian mixtures)", "recipes": recipes}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main_build():
     """Index build and insert throughput: --n rows (default 1M) x 128, integer-valued, 1,000
     clusters, R=64 L=100 alpha=1.2, built in batches of 10,000 with the exact uint8 copy
@@ -1083,4 +1140,6 @@ if __name__ == "__main__":
             sys.exit(main_serve())
         if cfg == "build":
             sys.exit(main_build())
+        if cfg == "pq":
+            sys.exit(main_pq())
     sys.exit(main())

@@ -73,7 +73,7 @@ __device__ __forceinline__ uint32_t bloom_pack(uint32_t x) { return (bloom_h1(x)
 // per instruction).
 struct StoreF32 {
     static constexpr int  kElems = 4, kLanes128 = 32, kM = 8;
-    static constexpr bool kScaled = false, kInt = false;
+    static constexpr bool kScaled = false, kInt = false, kPQ = false;
     __device__ __forceinline__ static void widen2(const uint4& r, float2 (&o)[2]) {
         o[0] = make_float2(__uint_as_float(r.x), __uint_as_float(r.y));
         o[1] = make_float2(__uint_as_float(r.z), __uint_as_float(r.w));
@@ -81,7 +81,7 @@ struct StoreF32 {
 };
 struct StoreBF16 {
     static constexpr int  kElems = 8, kLanes128 = 16, kM = 8;
-    static constexpr bool kScaled = false, kInt = false;
+    static constexpr bool kScaled = false, kInt = false, kPQ = false;
     // a BF16 is the upper half of its FP32 value
     __device__ __forceinline__ static void widen2(const uint4& r, float2 (&o)[4]) {
         const uint32_t w[4] = {r.x, r.y, r.z, r.w};
@@ -91,7 +91,7 @@ struct StoreBF16 {
 };
 struct StoreFP8 {
     static constexpr int  kElems = 16, kLanes128 = 8, kM = 8;
-    static constexpr bool kScaled = true, kInt = false;
+    static constexpr bool kScaled = true, kInt = false, kPQ = false;
     // the 16 codes of a chunk, unscaled: one e4m3x2 -> f16x2 conversion per pair,
     // then f16 -> f32 (both exact)
     __device__ __forceinline__ static void codes2(const uint4& r, float2 (&o)[8]) {
@@ -107,7 +107,7 @@ struct StoreFP8 {
 };
 struct StoreU8 {
     static constexpr int  kElems = 16, kLanes128 = 8, kM = 8;
-    static constexpr bool kScaled = false, kInt = true;  // exact dp4a path for integer queries
+    static constexpr bool kScaled = false, kInt = true, kPQ = false;  // exact dp4a path for integer queries
     __device__ __forceinline__ static void widen(const uint4& r, float (&o)[16]) {
         const uint32_t w[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
@@ -119,6 +119,15 @@ struct StoreU8 {
         }
     }
 };
+// Product-quantized codes (pq.cu): one byte per subspace of kPqSub = 8 dimensions,
+// so a 16-byte chunk holds the codes of 128 dimensions.  A row's distance is the
+// sum of its codes' entries in the query's table (one lane per 16 codes).
+struct StorePQ {
+    static constexpr int  kElems = 128, kLanes128 = 1, kM = 1;
+    static constexpr bool kScaled = false, kInt = false, kPQ = true;
+};
+constexpr uint32_t kPqSub = 8;    // dimensions per subspace
+constexpr uint32_t kPqK   = 256;  // centroids per subspace (one byte per code)
 
 // Lanes per row (kT), 16-byte chunks per lane (kCPL) and rows per lane (kM) of
 // store S in dimension class DC.  Integer rows of 128 bytes take 4 lanes of 2
@@ -159,8 +168,10 @@ template <typename S, int DC>
 struct Query {
     // FP32 copy of the lane's chunks as element pairs (integer stores keep none:
     // their rare non-integer fallback re-reads the row through L1)
-    float2       f2[S::kInt ? 1 : Layout<S, DC>::kCPL][S::kInt ? 1 : S::kElems / 2];
-    uint32_t     u[Layout<S, DC>::kCPL][S::kElems / 4];
+    float2       f2[S::kInt || S::kPQ ? 1 : Layout<S, DC>::kCPL][S::kInt || S::kPQ ? 1 : S::kElems / 2];
+    uint32_t     u[S::kPQ ? 1 : Layout<S, DC>::kCPL][S::kPQ ? 1 : S::kElems / 4];
+    const uint16_t* lut;        // PQ: this warp's distance table [D / 8][256] in shared memory
+    float           lut_scale;  // PQ: distance = scale * sum of table entries
     const float* row;
     int          qq;
     float        qn;  // this lane's share of |q|^2 (scaled stores)
@@ -172,6 +183,11 @@ struct Query {
 template <typename S, int DC>
 __device__ __forceinline__ void load_query(Query<S, DC>& q, const float* row, uint32_t D, uint32_t lane,
                                            const float* center = nullptr) {
+    if constexpr (S::kPQ) {  // the PQ query is its distance table (build_pq_lut)
+        q.row  = row;
+        q.qint = false;
+        return;
+    }
     using Ly              = Layout<S, DC>;
     const uint32_t chunks = D / S::kElems;
     const uint32_t t      = lane % Ly::kT;
@@ -278,7 +294,7 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
     using Ly                 = Layout<S, DC>;
     constexpr int  M         = Ly::kM;
     const uint32_t chunks    = D / S::kElems;
-    const uint64_t row_bytes = (uint64_t)D * (16 / S::kElems);
+    const uint64_t row_bytes = (uint64_t)D * 16u / (uint64_t)S::kElems;
     const uint32_t t         = lane % Ly::kT;
     const uint32_t g         = lane / Ly::kT;
     uint4          x[M][Ly::kCPL];
@@ -314,6 +330,27 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
         }
         if constexpr (S::kScaled) sc[m] = valid ? __ldg(scale + id) : make_float2(0.f, 0.f);
         else sc[m] = make_float2(1.f, 0.f);
+    }
+    if constexpr (S::kPQ) {
+        // lane t of a group holds the codes of subspaces 16 t .. 16 t + 15 (none when
+        // its chunk lies past the row: D = 384 in the 512-dimension class)
+        float          v[M];
+        const uint32_t k0 = Ly::chunk(t, 0);
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            uint32_t acc = 0;
+            if (k0 < chunks) {
+                const uint16_t* tb   = q.lut + 16u * kPqK * k0;
+                const unsigned  w[4] = {x[m][0].x, x[m][0].y, x[m][0].z, x[m][0].w};
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) acc += tb[(4u * i + b) * kPqK + ((w[i] >> (8 * b)) & 0xffu)];
+                }
+            }
+            v[m] = (float)acc;  // <= 16 * 65535: exact
+        }
+        return group_reduce<M, Ly::kT, float>(v, lane) * q.lut_scale;
     }
     if constexpr (S::kInt) {
         if (q.qint) {
@@ -363,7 +400,7 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
         }
         // rounding can leave a tiny negative for a row equal to the query
         return fmaxf(group_reduce<M, Ly::kT, float>(v, lane), 0.f);
-    } else if constexpr (!S::kInt) {
+    } else if constexpr (!S::kInt && !S::kPQ) {
         float v[M];
         // (x - q)^2 on element pairs: x - q = fma(q, -1, x), then fma(d, d, acc)
         const float2 neg1 = make_float2(-1.f, -1.f);
@@ -386,7 +423,7 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
 #pragma unroll
         for (int m = 0; m < M; ++m) v[m] = acc[m].x + acc[m].y;
         return group_reduce<M, Ly::kT, float>(v, lane);
-    } else {
+    } else if constexpr (S::kInt) {
         // integer rows with a query that is not (rare): FP32 from the row bytes and
         // the query re-read through L1
         float v[M];
@@ -415,6 +452,59 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
         }
         return group_reduce<M, Ly::kT, float>(v, lane);
     }
+}
+
+// The PQ distance table of one query, built by its warp into `lut` (shared memory,
+// [D / 8][256] u16): entry (m, k) = ||q_m - c_mk||^2 / scale, rounded, with one scale
+// per query from a bound on every entry, (||q_m|| + max_k ||c_mk||)^2 <= 65535 scale.
+// cb: [D / 8][256][8] centroids; cnorm: [D / 8] largest centroid norm per subspace.
+template <int DC>
+__device__ __forceinline__ void build_pq_lut(Query<StorePQ, DC>& q, uint16_t* lut, const float* cb,
+                                             const float* cnorm, const float* row, uint32_t D, uint32_t lane) {
+    const uint32_t M     = D / kPqSub;
+    float          bound = 0.f;
+    for (uint32_t m = lane; m < M; m += 32) {
+        const float4 a  = __ldg(reinterpret_cast<const float4*>(row + kPqSub * m));
+        const float4 b  = __ldg(reinterpret_cast<const float4*>(row + kPqSub * m) + 1);
+        const float  qn = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z + a.w * a.w + b.x * b.x + b.y * b.y +
+                                b.z * b.z + b.w * b.w);
+        const float  bm = qn + __ldg(cnorm + m);
+        bound           = fmaxf(bound, bm * bm);
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) bound = fmaxf(bound, __shfl_xor_sync(0xffffffffu, bound, o));
+    const float scale = bound > 0.f ? bound / 65535.f : 1.f;
+    const float inv   = 1.f / scale;
+    for (uint32_t e = lane; e < M * kPqK; e += 32) {
+        const uint32_t m  = e / kPqK;
+        const float4   qa = __ldg(reinterpret_cast<const float4*>(row + kPqSub * m));
+        const float4   qb = __ldg(reinterpret_cast<const float4*>(row + kPqSub * m) + 1);
+        const float4   ca = __ldg(reinterpret_cast<const float4*>(cb + (uint64_t)kPqSub * e));
+        const float4   cc = __ldg(reinterpret_cast<const float4*>(cb + (uint64_t)kPqSub * e) + 1);
+        float          d  = 0.f;
+        d                 = sqdiff(qa.x, ca.x, d);
+        d                 = sqdiff(qa.y, ca.y, d);
+        d                 = sqdiff(qa.z, ca.z, d);
+        d                 = sqdiff(qa.w, ca.w, d);
+        d                 = sqdiff(qb.x, cc.x, d);
+        d                 = sqdiff(qb.y, cc.y, d);
+        d                 = sqdiff(qb.z, cc.z, d);
+        d                 = sqdiff(qb.w, cc.w, d);
+        lut[e]            = (uint16_t)fminf(65535.f, rintf(d * inv));
+    }
+    __syncwarp();
+    q.lut       = lut;
+    q.lut_scale = scale;
+}
+
+// Exponent e with |x| < 2^e for every x of a column whose largest magnitude has
+// these float bits (0 for an all-zero column): the column's fixed-point grid is
+// 2^(e - B) (exact integer sums of the medoid's column means and of PQ centroids).
+__device__ __forceinline__ int column_exponent(uint32_t bound_bits) {
+    if (bound_bits == 0u) return 0;
+    int e = 0;
+    frexpf(__uint_as_float(bound_bits), &e);  // bound < 2^e
+    return e;
 }
 
 // ---------------------------------------------------------------- launches

@@ -182,12 +182,6 @@ cudaError_t launch_set_bits(uint32_t* bits, const uint32_t* ids, uint64_t n, uin
 // integers, which is exact.  For integer-valued rows every term is exact and the
 // means equal a sequential FP64 sum divided by n.  The squared distances to the
 // mean are summed sequentially over d without contraction (as the oracle does).
-__device__ __forceinline__ int column_exponent(uint32_t bound_bits) {
-    if (bound_bits == 0u) return 0;
-    int e = 0;
-    frexpf(__uint_as_float(bound_bits), &e);  // bound < 2^e
-    return e;
-}
 __global__ void col_bound_kernel(const float* vecs, uint64_t n, uint32_t D, uint32_t* bound) {
     const uint32_t d = threadIdx.x + blockIdx.y * blockDim.x;
     if (d >= D) return;
@@ -238,6 +232,14 @@ unsigned long long* medoid_best(void* ws, uint32_t D) {
     return reinterpret_cast<unsigned long long*>(static_cast<char*>(ws) + align16(sizeof(double) * D) +
                                                  align16(sizeof(uint32_t) * D));
 }
+cudaError_t launch_col_bounds(const float* vecs, uint64_t n, uint32_t D, uint32_t* bound, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(bound, 0, sizeof(uint32_t) * D, st);
+    if (e != cudaSuccess || n == 0) return e;
+    const dim3 g((unsigned)((n + 1023) / 1024), (D + 127) / 128);
+    col_bound_kernel<<<g, 128, 0, st>>>(vecs, n, D, bound);
+    return cudaGetLastError();
+}
+
 static cudaError_t launch_col_means_f64(const float* vecs, uint64_t n, uint32_t D, void* ws, cudaStream_t st) {
     auto* sum   = static_cast<unsigned long long*>(ws);
     auto* bound = reinterpret_cast<uint32_t*>(static_cast<char*>(ws) + align16(sizeof(double) * D));

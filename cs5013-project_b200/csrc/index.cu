@@ -205,9 +205,11 @@ struct vann_index {
     bool        consistent = false;
 
     float*    vecs  = nullptr;
-    void*     store[4] = {nullptr, nullptr, nullptr, nullptr};
+    void*     store[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // by vann_store
     float2*   fp8_scale = nullptr;  // per row (scale, scale^2 |codes|^2)
     float*    fp8_center = nullptr; // per dimension: the FP8 codes encode row - center
+    float*    pq_cb = nullptr;      // PQ copy: [D / 8][256][8] centroids
+    float*    pq_cnorm = nullptr;   // PQ copy: [D / 8] largest centroid norm per subspace
     uint32_t* deg  = nullptr;
     uint32_t* adj  = nullptr;
     uint32_t* adj_h = nullptr;  // packed filter slots beside every adjacency entry
@@ -249,6 +251,8 @@ struct vann_index {
         for (void* s : store) cudaFree(s);
         cudaFree(fp8_scale);
         cudaFree(fp8_center);
+        cudaFree(pq_cb);
+        cudaFree(pq_cnorm);
         cudaFree(deg);
         cudaFree(adj);
         cudaFree(adj_h);
@@ -339,6 +343,18 @@ struct vann_index {
             void*  dst = static_cast<char*>(store[s]) + first * p.dim * esz;
             VCHECK(vann::launch_convert(vecs + first * p.dim, dst, s == 2 ? fp8_scale + first : nullptr,
                                         s == 2 ? fp8_center : nullptr, rows, p.dim, s, u8_inexact(), st));
+        }
+        if (store[4] && rows > 0) {
+            // PQ: the codebook is trained on the rows that replace every row, then fixed
+            if (first == 0) {
+                DevBuf ws;
+                ws.ensure(vann::pq_train_ws_bytes(rows, p.dim));
+                VCHECK(vann::launch_pq_train(vecs, rows, p.dim, pq_cb, pq_cnorm, ws.p, st));
+                VCHECK(cudaStreamSynchronize(st));  // the workspace is freed below
+                ws.release();
+            }
+            VCHECK(vann::launch_pq_encode(vecs, first, rows, nullptr, p.dim, pq_cb, static_cast<uint8_t*>(store[4]),
+                                          st));
         }
     }
 
@@ -648,6 +664,8 @@ vann_status vann_create(const vann_params* params, vann_index** out) {
                  "the bf16 copy needs dim to be a multiple of 8");
         VREQUIRE(!(p.stores & ((1u << VANN_STORE_FP8) | (1u << VANN_STORE_U8))) || p.dim % 16 == 0,
                  VANN_ERR_UNSUPPORTED, "one-byte copies need dim to be a multiple of 16");
+        VREQUIRE(!(p.stores & (1u << VANN_STORE_PQ)) || p.dim % 128 == 0, VANN_ERR_UNSUPPORTED,
+                 "the PQ copy needs dim to be a multiple of 128");
         auto* h = new vann_index();
         try {
             h->p = p;
@@ -662,6 +680,11 @@ vann_status vann_create(const vann_params* params, vann_index** out) {
                 h->alloc((void**)&h->fp8_center, sizeof(float) * p.dim);
             }
             if (p.stores & (1u << VANN_STORE_U8)) h->alloc(&h->store[3], 1ull * C * p.dim);
+            if (p.stores & (1u << VANN_STORE_PQ)) {
+                h->alloc(&h->store[4], 1ull * C * (p.dim / vann::kPqSub));
+                h->alloc((void**)&h->pq_cb, sizeof(float) * (size_t)p.dim * vann::kPqK);
+                h->alloc((void**)&h->pq_cnorm, sizeof(float) * (p.dim / vann::kPqSub));
+            }
             h->store[0] = h->vecs;
             h->alloc((void**)&h->deg, sizeof(uint32_t) * C);
             h->alloc((void**)&h->adj, sizeof(uint32_t) * C * p.degree);
@@ -985,7 +1008,7 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
                  "null argument");
         VREQUIRE(sp->k >= 1 && sp->L >= sp->k && sp->L <= 1024, VANN_ERR_INVALID,
                  "need 1 <= k <= L <= 1024");
-        VREQUIRE(sp->store < 4 && h->store[sp->store] != nullptr, VANN_ERR_UNSUPPORTED,
+        VREQUIRE(sp->store < 5 && h->store[sp->store] != nullptr, VANN_ERR_UNSUPPORTED,
                  "requested store was not enabled at create");
         VREQUIRE(sp->beam <= 2, VANN_ERR_INVALID, "beam must be 0, 1 or 2");
         VREQUIRE(sp->beam < 2 || (sp->L <= 64 && h->p.dim <= 128 && h->p.degree <= 64), VANN_ERR_UNSUPPORTED,
@@ -997,6 +1020,8 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
         a.store = h->store[sp->store];
         a.scale = h->fp8_scale;
         a.center = sp->store == VANN_STORE_FP8 ? h->fp8_center : nullptr;
+        a.pq_cb = h->pq_cb;
+        a.pq_cnorm = h->pq_cnorm;
         a.vecs_f32 = h->vecs;
         a.deg = h->deg;
         a.adj = h->adj;
@@ -1203,6 +1228,9 @@ vann_status vann_insert(vann_index* h, const float* d_vecs, uint64_t n, uint32_t
                     VCHECK(vann::launch_convert_ids(h->vecs, h->nodes.as<uint32_t>(), n, h->store[s],
                                                     s == 2 ? h->fp8_scale : nullptr, s == 2 ? h->fp8_center : nullptr,
                                                     D, s, h->u8_inexact(), st));
+            if (h->store[4])
+                VCHECK(vann::launch_pq_encode(h->vecs, 0, n, h->nodes.as<uint32_t>(), D, h->pq_cb,
+                                              static_cast<uint8_t*>(h->store[4]), st));
         }
         h->size += n - reuse;
         const bool parity = (h->p.flags & VANN_QUIRK_SKIP_BATCH_INDEX) != 0;

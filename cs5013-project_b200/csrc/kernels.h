@@ -15,6 +15,8 @@ struct SearchArgs {
     const void*     store;     // traversal copy (F32 / BF16 / FP8 / U8 rows)
     const float2*   scale;     // FP8 copy: per row (scale, scale^2 * |codes|^2)
     const float*    center;    // FP8 copy: per-dimension centre the codes are relative to
+    const float*    pq_cb;     // PQ copy: [D / 8][256][8] centroids
+    const float*    pq_cnorm;  // PQ copy: [D / 8] largest centroid norm per subspace
     const float*    vecs_f32;  // exact rows (rerank)
     const uint32_t* deg;
     const uint32_t* adj;
@@ -129,6 +131,16 @@ cudaError_t launch_convert(const float* src, void* dst, float2* scale, const flo
                            uint32_t D, int store, uint32_t* inexact, cudaStream_t st);
 cudaError_t launch_convert_ids(const float* vecs, const uint32_t* ids, uint64_t n, void* dst, float2* scale,
                                const float* center, uint32_t D, int store, uint32_t* inexact, cudaStream_t st);
+// float bits of each column's largest magnitude over rows 0 .. n-1
+cudaError_t launch_col_bounds(const float* vecs, uint64_t n, uint32_t D, uint32_t* bound, cudaStream_t st);
+// PQ codebook (pq.cu): cb [D / 8][256][8] centroids trained on rows 0 .. n-1, cnorm [D / 8]
+// largest centroid norm per subspace; ws: pq_train_ws_bytes(n, D).  D % 128 == 0.
+size_t      pq_train_ws_bytes(uint64_t n, uint32_t D);
+cudaError_t launch_pq_train(const float* vecs, uint64_t n, uint32_t D, float* cb, float* cnorm, void* ws,
+                            cudaStream_t st);
+// codes [row][D / 8] of rows first .. first + rows - 1, or of rows ids[0 .. rows) when ids is set
+cudaError_t launch_pq_encode(const float* vecs, uint64_t first, uint64_t rows, const uint32_t* ids, uint32_t D,
+                             const float* cb, uint8_t* codes, cudaStream_t st);
 // FP32 column means of rows 0 .. n-1 (the medoid's exact column sums); ws: medoid_ws_bytes(D)
 cudaError_t launch_col_mean(const float* vecs, uint64_t n, uint32_t D, void* ws, float* mean, cudaStream_t st);
 cudaError_t launch_iota(uint32_t* out, uint64_t n, uint32_t first, cudaStream_t st);

@@ -23,8 +23,9 @@ struct SmemLayout {
     uint32_t lp;      // L rounded up to 32
     uint32_t maxr;    // neighbour slots
     uint32_t keys;    // rerank key slots (power of two) or 0
+    uint32_t lut;     // offset of the PQ distance table (lut_bytes, 0 for other stores)
     uint32_t bytes;   // per warp
-    __host__ __device__ static SmemLayout make(uint32_t L, uint32_t maxr, bool rerank) {
+    __host__ __device__ static SmemLayout make(uint32_t L, uint32_t maxr, bool rerank, uint32_t lut_bytes = 0) {
         SmemLayout s;
         s.lp   = (L + 31u) & ~31u;
         s.maxr = maxr;
@@ -34,7 +35,8 @@ struct SmemLayout {
             while (p < s.lp) p <<= 1;
             s.keys = p;
         }
-        s.bytes = 5008u + 8u * s.lp + 8u * s.maxr + 8u * s.keys;
+        s.lut   = 5008u + 8u * s.lp + 8u * s.maxr + 8u * s.keys;
+        s.bytes = s.lut + lut_bytes;
         return s;
     }
 };
@@ -68,7 +70,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
     constexpr int    G     = Layout<S, DC>::kG;
     const uint32_t   lane  = threadIdx.x & 31u;
     const uint32_t   wib   = threadIdx.x >> 5;
-    const SmemLayout lay   = SmemLayout::make(a.L, SPL * 32, a.rerank != 0);
+    const SmemLayout lay   = SmemLayout::make(a.L, SPL * 32, a.rerank != 0, S::kPQ ? 64u * a.D : 0u);
     unsigned char*   base  = smem + (size_t)wib * lay.bytes;
     uint32_t*        bloom = reinterpret_cast<uint32_t*>(base);
     uint32_t*        wl_id = reinterpret_cast<uint32_t*>(base + 5008);
@@ -92,6 +94,9 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
 
         Query<S, DC> qv;
         load_query<S, DC>(qv, a.queries + (uint64_t)q * a.D, a.D, lane, a.center);
+        if constexpr (S::kPQ)
+            build_pq_lut<DC>(qv, reinterpret_cast<uint16_t*>(base + lay.lut), a.pq_cb, a.pq_cnorm,
+                             a.queries + (uint64_t)q * a.D, a.D, lane);
         for (uint32_t w = lane; w < kBloomWords; w += 32) bloom[w] = 0u;
 
         uint32_t skip = kNone;
@@ -371,7 +376,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
 
 template <typename S, int DC, int SPL, int MINB>
 static cudaError_t launch_t(const SearchArgs& a, int num_sms, cudaStream_t st) {
-    SmemLayout lay   = SmemLayout::make(a.L, SPL * 32, a.rerank != 0);
+    SmemLayout lay   = SmemLayout::make(a.L, SPL * 32, a.rerank != 0, S::kPQ ? 64u * a.D : 0u);
     const int  warps = 4;
     size_t     smem  = (size_t)lay.bytes * warps;
     auto       kern  = search_kernel<S, DC, SPL, MINB>;

@@ -25,11 +25,13 @@ constexpr uint64_t kSentinel = ~0ull;
 
 struct RegLayout {
     uint32_t maxr;   // candidate slots (>= 64 so that the rerank ids fit too)
-    uint32_t bytes;  // per warp: bloom filter + candidate ids/distances + 64 merge payloads
-    __host__ __device__ static RegLayout make(uint32_t slots) {
+    uint32_t lut;    // offset of the PQ distance table (lut_bytes of them, 0 for other stores)
+    uint32_t bytes;  // per warp: bloom filter + candidate ids/distances + 64 merge payloads + table
+    __host__ __device__ static RegLayout make(uint32_t slots, uint32_t lut_bytes = 0) {
         RegLayout l;
         l.maxr  = slots < 64u ? 64u : slots;
-        l.bytes = 5008u + 8u * l.maxr + 256u;
+        l.lut   = 5008u + 8u * l.maxr + 256u;
+        l.bytes = l.lut + lut_bytes;
         return l;
     }
 };
@@ -148,7 +150,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
     constexpr int   NS    = BEAM * SPL;  // neighbour slots per lane in one hop
     const uint32_t  lane  = threadIdx.x & 31u;
     const uint32_t  wib   = threadIdx.x >> 5;
-    const RegLayout lay   = RegLayout::make(NS * 32);
+    const RegLayout lay   = RegLayout::make(NS * 32, S::kPQ ? 64u * a.D : 0u);
     unsigned char*  base  = smem + (size_t)wib * lay.bytes;
     uint32_t*       bloom = reinterpret_cast<uint32_t*>(base);
     uint32_t*       nb_id = reinterpret_cast<uint32_t*>(base + 5008);
@@ -171,6 +173,9 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
 
         Query<S, DC> qv;
         load_query<S, DC>(qv, a.queries + (uint64_t)q * a.D, a.D, lane, a.center);
+        if constexpr (S::kPQ)
+            build_pq_lut<DC>(qv, reinterpret_cast<uint16_t*>(base + lay.lut), a.pq_cb, a.pq_cnorm,
+                             a.queries + (uint64_t)q * a.D, a.D, lane);
         for (uint32_t w = lane; w < kBloomWords; w += 32) bloom[w] = 0u;
 
         uint32_t skip = kNone;
@@ -474,7 +479,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
 
 template <typename S, int DC, int SPL, int LREG, int MINB, int BEAM = 1>
 static cudaError_t launch_rw(const SearchArgs& a, int num_sms, cudaStream_t st) {
-    RegLayout  lay   = RegLayout::make(BEAM * SPL * 32);
+    RegLayout  lay   = RegLayout::make(BEAM * SPL * 32, S::kPQ ? 64u * a.D : 0u);
     const int  warps = 4;
     size_t     smem  = (size_t)lay.bytes * warps;
     auto       kern  = search_kernel_rw<S, DC, SPL, LREG, MINB, BEAM>;

@@ -299,7 +299,7 @@ extern "C" {
 vann_status vann_server_create(vann_index* idx, const vann_server_params* params, vann_server** out) {
     if (!idx || !params || !out) return VANN_ERR_INVALID;
     const vann_server_params& p = *params;
-    if (p.max_batch == 0 || p.slots == 0 || p.max_k == 0 || p.max_k > 1024 || p.store > 3)
+    if (p.max_batch == 0 || p.slots == 0 || p.max_k == 0 || p.max_k > 1024 || p.store > 4)
         return VANN_ERR_INVALID;
     vann_info info{};
     vann_status st = vann_get_info(idx, &info);

@@ -21,8 +21,8 @@ LIB_PATH = os.path.join(_HERE, "libvann.so")
 
 OK, ERR_INVALID, ERR_CUDA, ERR_CAPACITY, ERR_IO, ERR_HOP_LIMIT = 0, 1, 2, 3, 4, 5
 ERR_NOT_FOUND, ERR_TIMEOUT, ERR_OOM, ERR_UNSUPPORTED, ERR_STATE = 6, 7, 8, 9, 10
-STORE_F32, STORE_BF16, STORE_FP8, STORE_U8 = 0, 1, 2, 3
-STORES = {"f32": STORE_F32, "bf16": STORE_BF16, "fp8": STORE_FP8, "u8": STORE_U8}
+STORE_F32, STORE_BF16, STORE_FP8, STORE_U8, STORE_PQ = 0, 1, 2, 3, 4
+STORES = {"f32": STORE_F32, "bf16": STORE_BF16, "fp8": STORE_FP8, "u8": STORE_U8, "pq": STORE_PQ}
 QUIRK_SKIP_BATCH_INDEX = 0x1
 NONE_ID = 0xFFFFFFFF
 STAGED_BIT = 0x80000000  # VANN_STAGED_ID(s): insert-list row s in vann_search_staged results

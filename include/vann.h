@@ -43,7 +43,12 @@ typedef enum {
     VANN_STORE_F32  = 0,
     VANN_STORE_BF16 = 1, /* round-to-nearest-even bf16, FP32 accumulation */
     VANN_STORE_FP8  = 2, /* e4m3 with one FP32 scale per vector (amax / 448) */
-    VANN_STORE_U8   = 3  /* uint8 codes; exact for integer data in [0, 255] */
+    VANN_STORE_U8   = 3, /* uint8 codes; exact for integer data in [0, 255] */
+    VANN_STORE_PQ   = 4  /* product-quantized codes: one byte per 8 dimensions (256
+                            k-means centroids per subspace), distances from a per-query
+                            table; approximate, meant for rerank = 1; dim a multiple
+                            of 128 (BANG's compressed traversal, bang_exact/src/
+                            parANN.cu:1107-1157) */
 } vann_store;
 
 /* Reference quirks, reproduced for parity when set. */
