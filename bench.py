@@ -373,35 +373,36 @@ def main():
 
     # ---- e2e through the public API with pinned host buffers.  Each step copies
     # its queries host->device, searches and copies ids/distances back.  Steps are
-    # pipelined as a serving loop runs them: an upload stream, two compute streams
-    # taking the steps in turn, and a download stream, so one step's copies overlap
-    # its neighbours' searches and the tail of one search (its last, longest
-    # queries) overlaps the start of the next.
+    # pipelined as a serving loop runs them: an upload stream, NPIPE compute streams
+    # taking the steps in turn and NPIPE buffer sets, and a download stream, so one
+    # step's copies overlap its neighbours' searches and the tail of one search (its
+    # last, longest queries) overlaps the next searches' start.
+    NPIPE = 3
     _, hs, hrr, hbeam = form_of[head]
     h_q = torch.from_numpy(q).pin_memory()
-    s_comp = [torch.cuda.Stream(), torch.cuda.Stream()]
+    s_comp = [torch.cuda.Stream() for _ in range(NPIPE)]
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
-    qbuf = [torch.empty_like(q_d) for _ in range(2)]
+    qbuf = [torch.empty_like(q_d) for _ in range(NPIPE)]
     obuf = [(torch.empty((nq, K), dtype=torch.int32, device=dev),
-             torch.empty((nq, K), dtype=torch.float32, device=dev)) for _ in range(2)]
+             torch.empty((nq, K), dtype=torch.float32, device=dev)) for _ in range(NPIPE)]
     h_out = [(torch.empty((nq, K), dtype=torch.int32).pin_memory(),
-              torch.empty((nq, K), dtype=torch.float32).pin_memory()) for _ in range(2)]
-    flushes = [flush, torch.empty_like(flush)]
-    ev_in = [torch.cuda.Event() for _ in range(2)]
-    ev_done = [torch.cuda.Event() for _ in range(2)]
-    ev_out = [torch.cuda.Event() for _ in range(2)]
+              torch.empty((nq, K), dtype=torch.float32).pin_memory()) for _ in range(NPIPE)]
+    flushes = [flush] + [torch.empty_like(flush) for _ in range(NPIPE - 1)]
+    ev_in = [torch.cuda.Event() for _ in range(NPIPE)]
+    ev_done = [torch.cuda.Event() for _ in range(NPIPE)]
+    ev_out = [torch.cuda.Event() for _ in range(NPIPE)]
 
     def e2e_run(nsteps):
         for i in range(nsteps):
-            bsel = i % 2
+            bsel = i % NPIPE
             sc = s_comp[bsel]
             with torch.cuda.stream(s_in):
-                if i >= 2:
+                if i >= NPIPE:
                     s_in.wait_event(ev_done[bsel])  # the search that read this buffer
                 qbuf[bsel].copy_(h_q, non_blocking=True)
                 ev_in[bsel].record(s_in)
             sc.wait_event(ev_in[bsel])
-            if i >= 2:
+            if i >= NPIPE:
                 sc.wait_event(ev_out[bsel])  # the download of this buffer's last results
             with torch.cuda.stream(sc):
                 flushes[bsel].zero_()  # an L2 flush (256 MB write) before every search
@@ -425,8 +426,8 @@ def main():
     e2e_ms = [e2e_total_ms / steps] * steps
     e2e_qps = nq * steps / (e2e_total_ms / 1e3)
     torch.cuda.synchronize()
-    got = h_out[(steps - 1) % 2][0][:, :K].to(torch.int64)
-    assert torch.equal(got, obuf[(steps - 1) % 2][0].cpu().to(torch.int64))
+    got = h_out[(steps - 1) % NPIPE][0][:, :K].to(torch.int64)
+    assert torch.equal(got, obuf[(steps - 1) % NPIPE][0].cpu().to(torch.int64))
 
     # ---- max over ranks
     total_s, e2e_total = max_over_ranks(torch, dist, [sum(hr["ms"]) / 1e3, sum(e2e_ms) / 1e3], dev)
@@ -486,9 +487,9 @@ def main():
             "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": nq * DIM * 4,
                     "d2h_bytes_per_step": nq * K * 8,
                     "how": "C ABI search on pinned host queries; per step H2D + L2 flush (256 MB write) + "
-                           "search + D2H; steps pipelined on an upload stream, two compute streams taking "
-                           "the steps in turn, and a download stream (a step's tail overlaps the next "
-                           "step's start, as in a serving loop)"},
+                           "search + D2H; steps pipelined on an upload stream, three compute streams (and "
+                           "buffer sets) taking the steps in turn, and a download stream (a step's tail "
+                           "overlaps the next steps' start, as in a serving loop)"},
             # per step: the search, and for a batch over 16 queries per SM the two kernels
             # that order it (entry distances, bucket order)
             "gpu_launches": steps * (3 if nq > 16 * torch.cuda.get_device_properties(dev).multi_processor_count
