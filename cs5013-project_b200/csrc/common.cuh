@@ -288,7 +288,11 @@ __device__ __forceinline__ bool round_writer(uint32_t lane) {
 // Integer stores skip the row slots m with no row in any lane (m * kP >= cnt,
 // a partial round): no loads and no arithmetic.  (The same branch around the
 // float stores' loads costs more than it saves.)
-template <typename S, int DC, typename IdFn>
+//
+// kIntQuery (integer stores): the caller knows the query is integer-valued (a row of
+// an exact uint8 copy), so the FP32 fallback for other queries is not compiled in;
+// its registers would otherwise set the kernel's count.
+template <typename S, int DC, bool kIntQuery = false, typename IdFn>
 __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* base, const float2* scale,
                                             IdFn ids, int cnt, uint32_t D, uint32_t lane) {
     using Ly                 = Layout<S, DC>;
@@ -353,7 +357,7 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
         return group_reduce<M, Ly::kT, float>(v, lane) * q.lut_scale;
     }
     if constexpr (S::kInt) {
-        if (q.qint) {
+        if (kIntQuery || q.qint) {
             int v[M];
 #pragma unroll
             for (int m = 0; m < M; ++m) {
@@ -423,34 +427,37 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
 #pragma unroll
         for (int m = 0; m < M; ++m) v[m] = acc[m].x + acc[m].y;
         return group_reduce<M, Ly::kT, float>(v, lane);
-    } else if constexpr (S::kInt) {
-        // integer rows with a query that is not (rare): FP32 from the row bytes and
-        // the query re-read through L1
+    } else if constexpr (S::kInt && !kIntQuery) {
+        // integer rows with a query that is not (rare): FP32 from the row bytes,
+        // gathered again here (so the registers of the loads above are free on this
+        // path and do not add to its peak), the query re-read through L1
         float v[M];
 #pragma unroll
-        for (int m = 0; m < M; ++m) v[m] = 0.f;
+        for (int m = 0; m < M; ++m) {
+            v[m]             = 0.f;
+            const int  r     = m * Ly::kP + (int)g;
+            const bool valid = r < cnt;
+            const uint32_t id = valid ? ids(r) : 0u;
 #pragma unroll
-        for (int c = 0; c < Ly::kCPL; ++c) {
-            const uint32_t k = Ly::chunk(t, c);
-            float          qf[S::kElems];
+            for (int c = 0; c < Ly::kCPL; ++c) {
+                const uint32_t k = Ly::chunk(t, c);
+                if (!valid || k >= chunks) continue;
+                const uint4    xr   = load16(base, row_bytes, id, k);
+                const uint32_t w4[4] = {xr.x, xr.y, xr.z, xr.w};
 #pragma unroll
-            for (int v4 = 0; v4 < S::kElems / 4; ++v4) {
-                float4 z = k < chunks ? __ldg(reinterpret_cast<const float4*>(q.row + k * S::kElems) + v4)
-                                      : make_float4(0.f, 0.f, 0.f, 0.f);
-                qf[4 * v4]     = z.x;
-                qf[4 * v4 + 1] = z.y;
-                qf[4 * v4 + 2] = z.z;
-                qf[4 * v4 + 3] = z.w;
-            }
-#pragma unroll
-            for (int m = 0; m < M; ++m) {
-                float e[S::kElems];
-                S::widen(x[m][c], e);
-#pragma unroll
-                for (int i = 0; i < S::kElems; ++i) v[m] = sqdiff(qf[i], e[i], v[m]);
+                for (int v4 = 0; v4 < S::kElems / 4; ++v4) {
+                    const float4   z = __ldg(reinterpret_cast<const float4*>(q.row + k * S::kElems) + v4);
+                    const uint32_t w = w4[v4];
+                    v[m]             = sqdiff(z.x, (float)(w & 0xffu), v[m]);
+                    v[m]             = sqdiff(z.y, (float)((w >> 8) & 0xffu), v[m]);
+                    v[m]             = sqdiff(z.z, (float)((w >> 16) & 0xffu), v[m]);
+                    v[m]             = sqdiff(z.w, (float)(w >> 24), v[m]);
+                }
             }
         }
         return group_reduce<M, Ly::kT, float>(v, lane);
+    } else {
+        return 0.f;  // not reached: an integer query took the dp4a path
     }
 }
 

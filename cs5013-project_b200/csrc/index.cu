@@ -460,8 +460,9 @@ struct vann_index {
         // exact uint8 rows give the FP32 distances bit for bit from a quarter of the bytes
         int sstore = VANN_STORE_F32;
         if (u8_exact(st)) {
-            a.store = store[3];
-            sstore  = VANN_STORE_U8;
+            a.store       = store[3];
+            sstore        = VANN_STORE_U8;
+            a.int_queries = 1;  // the batch's rows are rows of the exact copy
         }
         // the first large batch of each row format times the launch-bound variants
         // (the same search each time: the expansion lists do not depend on the variant)

@@ -32,6 +32,7 @@ struct SearchArgs {
     uint32_t        skip_mode;  // 0 none, 1 batch index, 2 skip_base + batch index
     uint32_t        skip_base;
     uint32_t        beam;       // parents expanded per hop: 0/1 (the reference's search) or 2
+    int             int_queries; // every query is a row of the exact uint8 copy (build / insert)
     int             rerank;
     uint32_t*       out_ids;    // nq x k or null
     float*          out_d;

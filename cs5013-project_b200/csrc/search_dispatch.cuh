@@ -36,6 +36,19 @@ static cudaError_t launch_v(const SearchArgs& a, int variant, int sms, cudaStrea
                                : launch_rw_v<S, DC, SPL, 2, 1>(a, variant, sms, st);
     }
     if (a.beam == 2) return cudaErrorInvalidValue;
+    if constexpr (S::kInt && DC == 0 && SPL <= 2) {
+        if (a.int_queries) {  // build and insert searches over the exact uint8 copy
+            switch (variant) {
+                case 1: return launch_t<S, DC, SPL, 4, true>(a, sms, st);
+                case 2: return launch_t<S, DC, SPL, 5, true>(a, sms, st);
+                case 3: return launch_t<S, DC, SPL, 7, true>(a, sms, st);
+                case 4: return launch_t<S, DC, SPL, 8, true>(a, sms, st);
+                case 5: return launch_t<S, DC, SPL, 9, true>(a, sms, st);
+                case 6: return launch_t<S, DC, SPL, 10, true>(a, sms, st);
+                default: return launch_t<S, DC, SPL, 6, true>(a, sms, st);
+            }
+        }
+    }
     if constexpr (DC == 0 && SPL <= 2) {
         switch (variant) {
             case 1: return launch_t<S, DC, SPL, 4>(a, sms, st);

@@ -64,7 +64,9 @@ __device__ __forceinline__ uint32_t lower_bound_f(const float* a, uint32_t n, fl
     return lo;
 }
 
-template <typename S, int DC, int SPL, int MINB>
+// IQ: every query is a row of the exact uint8 copy (build and insert searches), so the
+// distance code for other queries is left out (fewer registers).
+template <typename S, int DC, int SPL, int MINB, bool IQ = false>
 __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int    G     = Layout<S, DC>::kG;
@@ -105,7 +107,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
 
         // initializeWorklist: entry visited, distance computed, not in the filter
         const uint32_t entry = a.entry;
-        float d0 = dist_group<S, DC>(qv, a.store, a.scale, [&](int) { return entry; }, 1, a.D, lane);
+        float d0 = dist_group<S, DC, IQ>(qv, a.store, a.scale, [&](int) { return entry; }, 1, a.D, lane);
         d0       = __shfl_sync(0xffffffffu, d0, 0);  // row 0 lives in lane 0
         if (lane == 0) {
             wl_id[0] = entry | kVisitedBit;
@@ -183,7 +185,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
             // distances: G rows per gather round, all loads of a round in flight
             for (uint32_t g0 = 0; g0 < cnt; g0 += G) {
                 int   gc = (int)min((uint32_t)G, cnt - g0);
-                float y  = dist_group<S, DC>(qv, a.store, a.scale,
+                float y  = dist_group<S, DC, IQ>(qv, a.store, a.scale,
                                              [&](int j) { return nb_id[g0 + j]; }, gc, a.D, lane);
                 uint32_t vi = round_row_of_lane<S, DC>(lane);
                 if (round_writer<S, DC>(lane) && (int)vi < gc) nb_d[g0 + vi] = y;
@@ -374,12 +376,12 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
     }
 }
 
-template <typename S, int DC, int SPL, int MINB>
+template <typename S, int DC, int SPL, int MINB, bool IQ = false>
 static cudaError_t launch_t(const SearchArgs& a, int num_sms, cudaStream_t st) {
     SmemLayout lay   = SmemLayout::make(a.L, SPL * 32, a.rerank != 0, S::kPQ ? 64u * a.D : 0u);
     const int  warps = 4;
     size_t     smem  = (size_t)lay.bytes * warps;
-    auto       kern  = search_kernel<S, DC, SPL, MINB>;
+    auto       kern  = search_kernel<S, DC, SPL, MINB, IQ>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
