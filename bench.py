@@ -346,7 +346,7 @@ def main():
     def algorithmic_bytes(name, hops, evals, adjw):
         _, store, rr, _ = form_of[name]
         s = {"f32": 4, "bf16": 2, "u8": 1, "fp8": 1}[store]
-        sc = 4 if store == "fp8" else 0
+        sc = 8 if store == "fp8" else 0  # the row's (scale, scaled code norm) pair
         L = results[name]["L"]
         per_q = (hops * 4 + adjw * 4 + evals * (DIM * s + sc) + 4 * DIM + 8 * K
                  + (min(L, 1 << 30) * 4 * DIM if rr else 0))
