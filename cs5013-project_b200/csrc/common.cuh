@@ -130,20 +130,21 @@ constexpr uint32_t kPqSub = 8;    // dimensions per subspace
 constexpr uint32_t kPqK   = 256;  // centroids per subspace (one byte per code)
 
 // Lanes per row (kT), 16-byte chunks per lane (kCPL) and rows per lane (kM) of
-// store S in dimension class DC.  Integer rows of 128 bytes take 4 lanes of 2
-// chunks and 4 rows each: half the row-id, address and cross-lane reduction work
-// of 8 lanes of one chunk, for the same 32 rows per gather round.
+// store S in dimension class DC.  In the smallest dimension class, integer, FP32
+// and BF16 rows give each lane two adjacent chunks (32 contiguous bytes, one
+// 256-bit load) and half the rows per round: the same rows per gather round for
+// half the row-id loads, addresses and cross-lane reduction levels.
 template <typename S, int DC>
 struct Layout {
     static constexpr int  kChunks = S::kLanes128 << DC;
-    static constexpr bool kNarrow = S::kInt && kChunks == 8;
-    static constexpr int  kT   = kNarrow ? 4 : (kChunks < 32 ? kChunks : 32);
+    static constexpr bool kNarrow = DC == 0 && kChunks >= 8 && (S::kInt || (!S::kScaled && !S::kPQ));
+    static constexpr int  kT   = kNarrow ? kChunks / 2 : (kChunks < 32 ? kChunks : 32);
     static constexpr int  kCPL = kChunks / kT;
-    static constexpr int  kP   = 32 / kT;              // rows per warp load
-    static constexpr int  kM   = kNarrow ? 4 : S::kM;  // rows per lane per round
-    static constexpr int  kG   = kM * kP;              // rows per gather round
-    // chunk c of lane group member t: integer rows of 128 bytes give each lane two
-    // adjacent chunks (32 contiguous bytes, one 256-bit load); the others interleave
+    static constexpr int  kP   = 32 / kT;                       // rows per warp load
+    static constexpr int  kM   = kNarrow ? S::kM / 2 : S::kM;   // rows per lane per round
+    static constexpr int  kG   = kM * kP;                       // rows per gather round
+    // chunk c of lane group member t: adjacent pairs in the narrow layout, else
+    // interleaved
     __device__ __forceinline__ static uint32_t chunk(uint32_t t, int c) {
         return kNarrow ? t * (uint32_t)kCPL + (uint32_t)c : t + (uint32_t)kT * (uint32_t)c;
     }
