@@ -347,11 +347,13 @@ struct vann_index {
         if (store[4] && rows > 0) {
             // PQ: the codebook is trained on the rows that replace every row, then fixed
             if (first == 0) {
-                DevBuf ws;
-                ws.ensure(vann::pq_train_ws_bytes(rows, p.dim));
-                VCHECK(vann::launch_pq_train(vecs, rows, p.dim, pq_cb, pq_cnorm, ws.p, st));
-                VCHECK(cudaStreamSynchronize(st));  // the workspace is freed below
-                ws.release();
+                struct Scratch {  // training workspace, freed on every way out
+                    DevBuf b;
+                    ~Scratch() { b.release(); }
+                } ws;
+                ws.b.ensure(vann::pq_train_ws_bytes(rows, p.dim));
+                VCHECK(vann::launch_pq_train(vecs, rows, p.dim, pq_cb, pq_cnorm, ws.b.p, st));
+                VCHECK(cudaStreamSynchronize(st));  // before the workspace is freed
             }
             VCHECK(vann::launch_pq_encode(vecs, first, rows, nullptr, p.dim, pq_cb, static_cast<uint8_t*>(store[4]),
                                           st));
