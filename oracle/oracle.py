@@ -64,6 +64,9 @@ def lib():
         L.vo_vamana_batch.restype = C.c_int
         L.vo_vamana_batch.argtypes = [C.POINTER(_Graph), C.c_int64, C.c_int64, C.c_int, C.c_float,
                                       C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.vo_vamana_batch_ids.restype = C.c_int
+        L.vo_vamana_batch_ids.argtypes = [C.POINTER(_Graph), C.c_void_p, C.c_int64, C.c_int, C.c_float,
+                                          C.c_uint32, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
         L.vo_consolidate.restype = C.c_int
         L.vo_consolidate.argtypes = [C.POINTER(_Graph), C.c_float, C.c_int, C.c_void_p, C.c_uint32,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
@@ -158,6 +161,15 @@ class Graph:
                                   C.byref(nf), threads)
         assert st == 0, st
         return int(ne.value), freed[: nf.value].copy()
+
+    def vamana_batch_ids(self, ids, L, alpha, entry, max_visited=600, max_reverse=500, skip_mode=0,
+                         bloom_mode=BLOOM_SNAPSHOT, threads=0):
+        """One Vamana batch over the node ids `ids` in that order (their rows already in
+        self.vecs, their degrees 0): inserts into reused ids."""
+        nodes = np.ascontiguousarray(ids, dtype=np.uint32)
+        g = self._c()
+        return lib().vo_vamana_batch_ids(C.byref(g), _p(nodes), len(nodes), L, alpha, entry, max_visited,
+                                         max_reverse, skip_mode, bloom_mode, threads)
 
     def vamana_batch(self, batch_start, batch_n, L, alpha, entry, max_visited=600, max_reverse=500,
                      skip_mode=1, bloom_mode=BLOOM_CHUNK32, threads=0):

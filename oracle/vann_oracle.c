@@ -298,14 +298,37 @@ static int sorted_out(const vo_graph* g, int64_t node, const float* node_vec, vo
 }
 
 /* ---------------------------------------------------------------- Vamana batch */
+/* The batch's node ids: nodes[b] when given, else batch_start + b. */
+static int batch_impl(vo_graph* g, const uint32_t* nodes, int64_t batch_start, int64_t batch_n, int L,
+                      float alpha, uint32_t entry, int max_visited, int max_reverse, int skip_mode,
+                      int bloom_mode, int threads);
+
 int vo_vamana_batch(vo_graph* g, int64_t batch_start, int64_t batch_n, int L, float alpha,
                     uint32_t entry, int max_visited, int max_reverse, int skip_mode,
                     int bloom_mode, int threads) {
+    if (batch_start < 0 || batch_n < 0 || batch_start + batch_n > g->n) return VO_ERR_INVALID;
+    return batch_impl(g, NULL, batch_start, batch_n, L, alpha, entry, max_visited, max_reverse, skip_mode,
+                      bloom_mode, threads);
+}
+
+/* A batch over any node ids (inserts into ids freed by a consolidation): the same steps,
+ * with the reverse entries of each target in batch order. */
+int vo_vamana_batch_ids(vo_graph* g, const uint32_t* nodes, int64_t batch_n, int L, float alpha,
+                        uint32_t entry, int max_visited, int max_reverse, int skip_mode, int bloom_mode,
+                        int threads) {
+    if (batch_n < 0 || (batch_n > 0 && !nodes)) return VO_ERR_INVALID;
+    for (int64_t b = 0; b < batch_n; ++b)
+        if (nodes[b] >= (uint64_t)g->n) return VO_ERR_INVALID;
+    return batch_impl(g, nodes, 0, batch_n, L, alpha, entry, max_visited, max_reverse, skip_mode, bloom_mode,
+                      threads);
+}
+
+static int batch_impl(vo_graph* g, const uint32_t* nodes, int64_t batch_start, int64_t batch_n, int L,
+                      float alpha, uint32_t entry, int max_visited, int max_reverse, int skip_mode,
+                      int bloom_mode, int threads) {
     const int     R = g->R, D = g->dim;
     const int64_t N = g->n;
-    if (batch_start < 0 || batch_n < 0 || batch_start + batch_n > N || L < 1 || R < 1 ||
-        max_visited < 1 || max_reverse < 1)
-        return VO_ERR_INVALID;
+    if (L < 1 || R < 1 || max_visited < 1 || max_reverse < 1) return VO_ERR_INVALID;
     if (threads <= 0) threads = omp_get_max_threads();
     int status = VO_OK;
 
@@ -319,7 +342,7 @@ int vo_vamana_batch(vo_graph* g, int64_t batch_start, int64_t batch_n, int L, fl
         float*    wd = (float*)malloc(sizeof(float) * (size_t)L);
 #pragma omp for schedule(dynamic, 16)
         for (int64_t b = 0; b < batch_n; ++b) {
-            int64_t  node = batch_start + b;
+            int64_t  node = (nodes ? (int64_t)nodes[b] : batch_start + b);
             uint32_t skip = skip_mode == 1   ? (uint32_t)b
                             : skip_mode == 2 ? (uint32_t)node
                                              : VO_NONE;
@@ -349,7 +372,7 @@ int vo_vamana_batch(vo_graph* g, int64_t batch_start, int64_t batch_n, int L, fl
         float*    cd = (float*)malloc(sizeof(float) * (size_t)max_visited);
 #pragma omp for schedule(dynamic, 16)
         for (int64_t b = 0; b < batch_n; ++b) {
-            int64_t      node = batch_start + b;
+            int64_t      node = (nodes ? (int64_t)nodes[b] : batch_start + b);
             const float* nv   = g->vecs + (size_t)node * D;
             int          na   = vis_n[b];
             for (int t = 0; t < na; ++t) {
@@ -373,7 +396,7 @@ int vo_vamana_batch(vo_graph* g, int64_t batch_start, int64_t batch_n, int L, fl
     uint32_t* rev   = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)N * max_reverse);
     uint32_t* rev_n = (uint32_t*)calloc((size_t)(N ? N : 1), sizeof(uint32_t));
     for (int64_t b = 0; b < batch_n; ++b) {
-        int64_t node  = batch_start + b;
+        int64_t node  = (nodes ? (int64_t)nodes[b] : batch_start + b);
         g->deg[node] = (uint32_t)chosen_n[b];
         for (int t = 0; t < chosen_n[b]; ++t) {
             uint32_t p                     = chosen[(size_t)b * R + t];

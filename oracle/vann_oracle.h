@@ -93,6 +93,13 @@ int vo_vamana_batch(vo_graph* g, int64_t batch_start, int64_t batch_n, int L, fl
 int vo_consolidate(vo_graph* g, float alpha, int cap, const unsigned char* is_free, uint32_t entry,
                    uint32_t* new_entry, uint32_t* freed, int64_t* n_freed, int threads);
 
+/* The same batch over the node ids nodes[0 .. batch_n) in that order (inserts into ids
+ * freed by a consolidation, taken from the free list): queries are those nodes' rows
+ * in g->vecs; reverse entries reach each target in batch order. */
+int vo_vamana_batch_ids(vo_graph* g, const uint32_t* nodes, int64_t batch_n, int L, float alpha,
+                        uint32_t entry, int max_visited, int max_reverse, int skip_mode, int bloom_mode,
+                        int threads);
+
 /* Deterministic random initial graph (hash-based, no self loops). */
 void vo_random_graph(int64_t n, int R, uint64_t seed, uint32_t* deg, uint32_t* adj);
 

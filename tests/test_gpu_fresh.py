@@ -116,3 +116,53 @@ def test_consolidate_bit_exact(oracle, vann_mod, fresh_graph, stores):
     extra = workload.mixture(5, 128, 30, seed=83)
     new = idx.insert(torch.from_numpy(extra).cuda()).cpu().numpy().tolist()
     assert new == freed_all[::-1][:5]
+
+
+@pytest.mark.parametrize("stores", [("f32",), ("f32", "u8")], ids=["cuda_cores", "tensor_cores"])
+def test_churn_cycle_bit_exact(oracle, vann_mod, fresh_graph, stores):
+    """The whole FreshVamana cycle, twice: lazy deletes, consolidation, then inserts in
+    uneven batches into the freed ids (the free list is a stack, last freed first).
+    After every insert batch the graph equals the oracle's, which runs the same batch
+    over the same ids (vo_vamana_batch_ids: search from the entry, out-prune, reverse
+    edges in batch order, re-prune)."""
+    import torch
+
+    base, g, entry = fresh_graph
+    n = base.shape[0]
+    idx = _index(vann_mod, base, g, entry, stores)
+    vecs = g.vecs.copy()
+    og = oracle.Graph(vecs, g.deg.copy(), g.adj.copy(), tomb=np.zeros((n + 31) // 32, np.uint32))
+    rng = np.random.default_rng(21)
+    dead_now = set()
+    is_free = np.zeros(n, np.uint8)
+    free_stack = []
+    o_entry = entry
+    for rnd in range(2):
+        live = np.array(sorted(set(range(n)) - dead_now))
+        dead = rng.choice(live, n * 6 // 100, replace=False)
+        dead_now |= set(dead.tolist())
+        og.tomb = oracle.tomb_bitmap(n, sorted(dead_now))
+        o_entry, freed = og.consolidate(1.2, 600, o_entry, is_free=is_free)
+        is_free[freed] = 1
+        free_stack.extend(freed.tolist())
+        idx.delete(torch.from_numpy(dead.astype(np.int32)).cuda())
+        idx.consolidate()
+        assert idx.info()["entry"] == o_entry, rnd
+        newv = workload.mixture(len(dead), 128, 30, seed=700 + rnd)
+        off = 0
+        for size in (37, 5, len(dead) - 42):
+            rows = newv[off:off + size]
+            off += size
+            want = [free_stack.pop() for _ in range(size)]
+            got = idx.insert(torch.from_numpy(rows).cuda()).cpu().numpy().tolist()
+            assert got == want, rnd
+            ids = np.array(want, np.uint32)
+            og.vecs[ids] = rows
+            og.deg[ids] = 0
+            for i in want:
+                og.tomb[i >> 5] &= np.uint32(~(1 << (i & 31)) & 0xFFFFFFFF)
+                is_free[i] = 0
+                dead_now.discard(i)
+            assert og.vamana_batch_ids(ids, 64, 1.2, o_entry, skip_mode=0) == 0
+            _, gdeg, gadj = idx.get_graph()
+            assert _rows_equal(gdeg, gadj, og.deg, og.adj) == [], (rnd, size)
