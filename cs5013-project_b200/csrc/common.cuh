@@ -17,6 +17,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 namespace vann {
 
 constexpr uint32_t kBloomSlots = 39988u;                 // bloom_filter.cuh:7
@@ -462,6 +464,16 @@ __device__ __forceinline__ float dist_group(const Query<S, DC>& q, const void* b
     }
 }
 
+// Squared L2 from the query to rows ids(0) .. ids(cnt-1), cnt <= kG, stored to
+// out[0 .. cnt).
+template <typename S, int DC, bool kIntQuery = false, typename IdFn>
+__device__ __forceinline__ void dist_round(const Query<S, DC>& q, const void* base, const float2* scale, IdFn ids,
+                                           int cnt, uint32_t D, uint32_t lane, float* out) {
+    const float    y  = dist_group<S, DC, kIntQuery>(q, base, scale, ids, cnt, D, lane);
+    const uint32_t vi = round_row_of_lane<S, DC>(lane);
+    if (round_writer<S, DC>(lane) && (int)vi < cnt) out[vi] = y;
+}
+
 // The PQ distance table of one query, built by its warp into `lut` (shared memory,
 // [D / 8][256] u16): entry (m, k) = ||q_m - c_mk||^2 / scale, rounded, with one scale
 // per query from a bound on every entry, (||q_m|| + max_k ||c_mk||)^2 <= 65535 scale.
@@ -542,6 +554,35 @@ inline cudaError_t fit_carveout(K kern, int threads, size_t smem, int* per_sm) {
                                     (int)cudaSharedmemCarveoutMaxShared);
     return cudaSuccess;
 }
+
+// kern<<<grid, block, smem, st>>>(args...).  With pdl, the launch is a programmatic
+// dependent of the kernel before it on the stream: its blocks may be scheduled once
+// every block of that kernel has executed griddepcontrol.launch_dependents (or
+// exited), so their launch overlaps its end; a dependent reads that kernel's output
+// only after griddepcontrol.wait, which returns when it has completed and its
+// writes are visible.  Without pdl, griddepcontrol.wait returns at once.
+template <typename... P, typename... A>
+inline cudaError_t launch_kernel(void (*kern)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, bool pdl,
+                                 A&&... args) {
+    if (!pdl) {
+        kern<<<grid, block, smem, st>>>(std::forward<A>(args)...);
+        return cudaGetLastError();
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim          = grid;
+    cfg.blockDim         = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream           = st;
+    cudaLaunchAttribute at[1];
+    at[0].id                                         = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs                                        = at;
+    cfg.numAttrs                                     = 1;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
+
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dependents_may_launch() { asm volatile("griddepcontrol.launch_dependents;"); }
 
 // ---------------------------------------------------------------- keys
 // Non-negative float distances order like their bit patterns.

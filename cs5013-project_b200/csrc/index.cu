@@ -82,6 +82,7 @@ struct DevBuf {
 // Squared FP32 distance from every query to the entry row (its float bits).
 __global__ void entry_dist_kernel(const float* queries, uint64_t nq, uint32_t D, const float* entry_row,
                                   uint32_t* keys) {
+    vann::grid_dependents_may_launch();  // the order kernel waits for the keys itself
     const uint64_t q    = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
     const uint32_t lane = threadIdx.x & 31u;
     if (q >= nq) return;
@@ -98,11 +99,18 @@ __global__ void entry_dist_kernel(const float* queries, uint64_t nq, uint32_t D,
 // One block orders the queries by distance to the entry point, farthest first, in
 // kOrderBuckets equal-width distance buckets (order within a bucket is whatever the
 // shared-memory atomics give: a schedule, not a result).  Two launches in all, where
-// a device-wide radix sort of a 10k batch takes several.
+// a device-wide radix sort of a 10k batch takes several.  It also zeroes the search's
+// query counter (when given one), which saves the search a memset node; launched
+// as a programmatic dependent of entry_dist_kernel, it starts while that kernel's
+// last blocks run and waits for their keys, and lets the search's blocks start
+// while it runs (they wait for it in turn).
 constexpr int kOrderThreads = 1024;
 constexpr int kOrderBuckets = 1024;
 __global__ void __launch_bounds__(kOrderThreads) order_by_bucket_kernel(const uint32_t* keys, uint32_t nq,
-                                                                        uint32_t* order) {
+                                                                        uint32_t* order, uint32_t* counter) {
+    vann::grid_dependency_wait();
+    vann::grid_dependents_may_launch();
+    if (counter != nullptr && threadIdx.x == 0) *counter = 0u;
     __shared__ uint32_t cnt[kOrderBuckets];
     __shared__ float    lo_w[32], hi_w[32];
     const uint32_t t = threadIdx.x;
@@ -267,9 +275,9 @@ struct vann_index {
             b->release();
     }
 
-    uint32_t* next_counter(cudaStream_t st) {
+    uint32_t* next_counter(cudaStream_t st, bool zero = true) {
         uint32_t* c = counters + (ring_pos++ % kCounterRing) * 32;
-        VCHECK(cudaMemsetAsync(c, 0, sizeof(uint32_t), st));
+        if (zero) VCHECK(cudaMemsetAsync(c, 0, sizeof(uint32_t), st));
         return c;
     }
 
@@ -286,14 +294,21 @@ struct vann_index {
     // index lives; and a search issued while its stream is being captured allocates
     // nothing: when the stream's workspace is too small, that batch runs in input
     // order, with the same results.
-    const uint32_t* search_order(const float* d_queries, uint64_t nq, cudaStream_t st) {
+    //
+    // counter (optional): the search's query counter, zeroed by the order kernel; the
+    // search may then be launched as its programmatic dependent (*pdl, false while the
+    // stream is being captured: a captured search keeps plain stream order).
+    const uint32_t* search_order(const float* d_queries, uint64_t nq, cudaStream_t st, uint32_t* counter = nullptr,
+                                 bool* pdl = nullptr) {
+        if (pdl) *pdl = false;
         if (nq <= 16ull * (uint64_t)num_sms || nq > 0x7FFFFFFFull) return nullptr;
-        const size_t need = sizeof(uint32_t) * 2 * nq;
-        DevBuf&      ob   = ord[st];
+        const size_t            need = sizeof(uint32_t) * 2 * nq;
+        DevBuf&                 ob   = ord[st];
+        cudaStreamCaptureStatus cs   = cudaStreamCaptureStatusNone;
+        VCHECK(cudaStreamIsCapturing(st, &cs));
+        const bool capturing = cs != cudaStreamCaptureStatusNone;
         if (ob.bytes < need) {
-            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-            VCHECK(cudaStreamIsCapturing(st, &cs));
-            if (cs != cudaStreamCaptureStatusNone) return nullptr;
+            if (capturing) return nullptr;
             if (ob.p) {
                 ord_retired.push_back(ob.p);
                 ob.p     = nullptr;
@@ -306,8 +321,10 @@ struct vann_index {
         entry_dist_kernel<<<(unsigned)((nq + 7) / 8), 256, 0, st>>>(d_queries, nq, p.dim,
                                                                   vecs + (uint64_t)entry * p.dim, keys);
         VCHECK(cudaGetLastError());
-        order_by_bucket_kernel<<<1, kOrderThreads, 0, st>>>(keys, (uint32_t)nq, order);
-        VCHECK(cudaGetLastError());
+        const bool chain = counter != nullptr && !capturing;
+        VCHECK(vann::launch_kernel(order_by_bucket_kernel, dim3(1), dim3(kOrderThreads), 0, st, chain, keys,
+                                   (uint32_t)nq, order, counter));
+        if (pdl) *pdl = chain;
         return order;
     }
 
@@ -1047,8 +1064,12 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
         a.adjw_out = d_adjw;
         a.Lq = h->pending_Lq;
         a.kq = h->pending_kq;
-        a.order = h->search_order(d_queries, nq, S(stream));
-        a.counter = h->next_counter(S(stream));
+        // the order kernel zeroes the counter, else a memset does
+        a.counter  = h->next_counter(S(stream), false);
+        bool chain = false;
+        a.order    = h->search_order(d_queries, nq, S(stream), a.counter, &chain);
+        if (a.order == nullptr) VCHECK(cudaMemsetAsync(a.counter, 0, sizeof(uint32_t), S(stream)));
+        a.pdl = chain ? 1 : 0;
         a.status = h->status;
         VCHECK(vann::launch_search(a, (int)sp->store, h->num_sms, S(stream), h->variant_for(*sp)));
     });

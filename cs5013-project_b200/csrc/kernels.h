@@ -44,7 +44,8 @@ struct SearchArgs {
     uint32_t*       evals_out;
     uint32_t*       adjw_out;   // per-query adjacency words read (sum of parent degrees)
     const uint32_t* order;      // order in which warps take the queries (a permutation) or null
-    uint32_t*       counter;    // zeroed before launch
+    uint32_t*       counter;    // zeroed before launch (by the order kernel when there is one)
+    int             pdl;        // launched as a programmatic dependent of the order kernel
     uint32_t*       status;
 };
 

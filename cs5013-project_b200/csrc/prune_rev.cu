@@ -49,10 +49,7 @@ __device__ __forceinline__ void dists_to(const float* qrow, const void* store, c
     for (uint32_t g0 = 0; g0 < nc; g0 += G) {
         const int      gc = (int)min((uint32_t)G, nc - g0);
         // uint8 rows are used only when every row is exact, so the query row is integer-valued
-        const float    y  = dist_group<S, DC, S::kInt>(q, store, nullptr, [&](int j) { return cid[g0 + j]; }, gc, D,
-                                                       lane);
-        const uint32_t vi = round_row_of_lane<S, DC>(lane);
-        if (round_writer<S, DC>(lane) && (int)vi < gc) out[g0 + vi] = y;
+        dist_round<S, DC, S::kInt>(q, store, nullptr, [&](int j) { return cid[g0 + j]; }, gc, D, lane, out + g0);
     }
 }
 

@@ -82,6 +82,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
     uint64_t*        nb_key = reinterpret_cast<uint64_t*>(nb_id);  // same bytes, after the ids/dists are read
     uint64_t*        keys  = reinterpret_cast<uint64_t*>(base + 5008 + 8 * lay.lp + 8 * lay.maxr);
     const uint32_t   R     = a.R;
+    grid_dependency_wait();  // the order kernel's order and counter
 
     for (;;) {
         uint32_t q = 0;
@@ -185,10 +186,8 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
             // distances: G rows per gather round, all loads of a round in flight
             for (uint32_t g0 = 0; g0 < cnt; g0 += G) {
                 int   gc = (int)min((uint32_t)G, cnt - g0);
-                float y  = dist_group<S, DC, IQ>(qv, a.store, a.scale,
-                                             [&](int j) { return nb_id[g0 + j]; }, gc, a.D, lane);
-                uint32_t vi = round_row_of_lane<S, DC>(lane);
-                if (round_writer<S, DC>(lane) && (int)vi < gc) nb_d[g0 + vi] = y;
+                dist_round<S, DC, IQ>(qv, a.store, a.scale, [&](int j) { return nb_id[g0 + j]; }, gc, a.D, lane,
+                                      nb_d + g0);
             }
             __syncwarp();
 
@@ -392,8 +391,7 @@ static cudaError_t launch_t(const SearchArgs& a, int num_sms, cudaStream_t st) {
     uint64_t grid = (uint64_t)per_sm * num_sms;
     if (grid > need) grid = need;
     if (grid == 0) return cudaSuccess;
-    kern<<<(unsigned)grid, warps * 32, smem, st>>>(a);
-    return cudaGetLastError();
+    return launch_kernel(kern, dim3((unsigned)grid), dim3(warps * 32), smem, st, a.pdl != 0, a);
 }
 
 }  // namespace vann
