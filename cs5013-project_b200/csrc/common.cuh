@@ -241,6 +241,51 @@ __device__ __forceinline__ void load_query(Query<S, DC>& q, const float* row, ui
     q.qq = qq;
 }
 
+// The query of an integer store taken straight from a row of the exact uint8 copy
+// (the caller knows every row there equals its FP32 row): the lane's chunks as
+// packed words, |q|^2 from dp4a.  The same Query as load_query gives for that FP32
+// row, from a quarter of the bytes and without the per-element checks.
+template <typename S, int DC>
+__device__ __forceinline__ void load_query_u8row(Query<S, DC>& q, const uint8_t* row, uint32_t D, uint32_t lane) {
+    static_assert(S::kInt, "uint8 rows");
+    using Ly                 = Layout<S, DC>;
+    const uint32_t chunks    = D / S::kElems;
+    const uint32_t t         = lane % Ly::kT;
+    uint32_t       qq        = 0;
+    uint4          w[Ly::kCPL];
+    if constexpr (Ly::kNarrow) {
+        const uint32_t k0 = Ly::chunk(t, 0);
+        if (k0 + 1u < chunks && (D & 31u) == 0u) {
+            load32(row, 0, 0, k0, w[0], w[1]);
+        } else {
+            w[0] = k0 < chunks ? load16(row, 0, 0, k0) : make_uint4(0u, 0u, 0u, 0u);
+            w[1] = k0 + 1u < chunks ? load16(row, 0, 0, k0 + 1u) : make_uint4(0u, 0u, 0u, 0u);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < Ly::kCPL; ++c) {
+            const uint32_t k = Ly::chunk(t, c);
+            w[c]             = k < chunks ? load16(row, 0, 0, k) : make_uint4(0u, 0u, 0u, 0u);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < Ly::kCPL; ++c) {
+        const uint32_t v[4] = {w[c].x, w[c].y, w[c].z, w[c].w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            q.u[c][i] = v[i];
+            qq        = __dp4a(v[i], v[i], qq);
+        }
+    }
+    int s = (int)qq;
+#pragma unroll
+    for (int o = Ly::kT / 2; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    q.qq   = s;
+    q.qn   = 0.f;
+    q.row  = nullptr;
+    q.qint = true;
+}
+
 __device__ __forceinline__ float sqdiff(float q, float x, float acc) {
     float d = q - x;
     return fmaf(d, d, acc);

@@ -39,26 +39,27 @@ struct RevWarp {  // shared memory of one warp
     uint32_t sb[kMaxA][kW];     // sorted positions of B candidates that prune A_i
 };
 
-// d(query row, candidate j) for every candidate j < nc into out[j]
+// d(row `qid`, candidate j) for every candidate j < nc into out[j]; the query comes
+// from the row format the distances use (uint8 rows: the exact uint8 row itself)
 template <typename S, int DC>
-__device__ __forceinline__ void dists_to(const float* qrow, const void* store, const uint32_t* cid, uint32_t nc,
-                                         float* out, uint32_t D, uint32_t lane) {
+__device__ __forceinline__ void dists_to(const PruneArgs& a, const void* store, uint32_t qid, const uint32_t* cid,
+                                         uint32_t nc, float* out, uint32_t lane) {
     Query<S, DC> q;
-    load_query<S, DC>(q, qrow, D, lane);
+    if constexpr (S::kInt) load_query_u8row<S, DC>(q, a.vecs_u8 + (uint64_t)qid * a.D, a.D, lane);
+    else load_query<S, DC>(q, a.vecs + (uint64_t)qid * a.D, a.D, lane);
     constexpr int G = Layout<S, DC>::kG;
     for (uint32_t g0 = 0; g0 < nc; g0 += G) {
-        const int      gc = (int)min((uint32_t)G, nc - g0);
+        const int gc = (int)min((uint32_t)G, nc - g0);
         // uint8 rows are used only when every row is exact, so the query row is integer-valued
-        dist_round<S, DC, S::kInt>(q, store, nullptr, [&](int j) { return cid[g0 + j]; }, gc, D, lane, out + g0);
+        dist_round<S, DC, S::kInt>(q, store, nullptr, [&](int j) { return cid[g0 + j]; }, gc, a.D, lane, out + g0);
     }
 }
 
 template <typename S, int DC>
 __device__ __forceinline__ void all_dists(const PruneArgs& a, const void* store, RevWarp& w, uint32_t node,
                                           uint32_t nA, uint32_t nc, uint32_t lane) {
-    dists_to<S, DC>(a.vecs + (uint64_t)node * a.D, store, w.cid, nc, w.cd, a.D, lane);
-    for (uint32_t i = 0; i < nA; ++i)
-        dists_to<S, DC>(a.vecs + (uint64_t)w.cid[i] * a.D, store, w.cid, nc, w.ad[i], a.D, lane);
+    dists_to<S, DC>(a, store, node, w.cid, nc, w.cd, lane);
+    for (uint32_t i = 0; i < nA; ++i) dists_to<S, DC>(a, store, w.cid[i], w.cid, nc, w.ad[i], lane);
 }
 
 // U8: distances from the exact uint8 rows (chosen on the host, which has read the
