@@ -10,7 +10,8 @@
 //
 //   1. one pass of gathers gives d(v, c) for every candidate; one more per A
 //      candidate gives d(a, c) (the rows are in L1 by then);
-//   2. the candidates are sorted by (distance, index) in shared memory;
+//   2. the candidates are ordered by (distance, index): B is already in that order
+//      (it is a RobustPrune selection), so the A candidates are merged in by rank;
 //   3. bit masks over the sorted positions: PA[i] = what A_i prunes,
 //      SB[i] = the B candidates that prune A_i;
 //   4. selection, all on those masks: every live B candidate ahead of the next
@@ -104,9 +105,41 @@ __global__ void __launch_bounds__(128) prune_rev_kernel(PruneArgs a, uint32_t* o
         // --- 2. stable order by (distance, candidate index)
         uint32_t p2 = 32;
         while (p2 < nc) p2 <<= 1;
-        for (uint32_t i = lane; i < p2; i += 32) w.keys[i] = i < nc ? make_key(w.cd[i], i) : ~0ull;
-        __syncwarp();
-        warp_bitonic_sort_smem(w.keys, p2, lane);
+        // B came out of RobustPrune in selection order: nondecreasing distance, ties in
+        // list order, which is also their index order here.  Then the order is B with
+        // the A candidates merged in (every A index is below every B index):
+        //   B_j goes to j + #{i : d(A_i) <= d(B_j)},
+        //   A_i to #{j : d(B_j) < d(A_i)} + #{k : (d(A_k), k) < (d(A_i), i)}.
+        // A list out of order (a graph set from outside) takes the bitonic sort.
+        bool in_order = true;
+        for (uint32_t j = lane; j + 1u < nB; j += 32) in_order &= w.cd[nA + j] <= w.cd[nA + j + 1u];
+        if (__all_sync(0xffffffffu, in_order)) {
+            for (uint32_t j = lane; j < nB; j += 32) {
+                const float d   = w.cd[nA + j];
+                uint32_t    pos = j;
+                for (uint32_t i = 0; i < nA; ++i) pos += w.cd[i] <= d ? 1u : 0u;
+                w.keys[pos] = make_key(d, nA + j);
+            }
+            for (uint32_t i = 0; i < nA; ++i) {
+                const float di  = w.cd[i];
+                uint32_t    pos = 0;
+                for (uint32_t j0 = 0; j0 < nB; j0 += 32) {
+                    const uint32_t j = j0 + lane;
+                    pos += __popc(__ballot_sync(0xffffffffu, j < nB && w.cd[nA + j] < di));
+                }
+                for (uint32_t k = 0; k < nA; ++k) {
+                    const float dk = w.cd[k];
+                    pos += (dk < di || (dk == di && k < i)) ? 1u : 0u;
+                }
+                if (lane == 0) w.keys[pos] = make_key(di, i);
+            }
+            for (uint32_t i = nc + lane; i < p2; i += 32) w.keys[i] = ~0ull;
+            __syncwarp();
+        } else {
+            for (uint32_t i = lane; i < p2; i += 32) w.keys[i] = i < nc ? make_key(w.cd[i], i) : ~0ull;
+            __syncwarp();
+            warp_bitonic_sort_smem(w.keys, p2, lane);
+        }
         const uint32_t m = min(nc, a.cap);
 
         // --- 3. masks over sorted positions t < m (position t = 32k + lane)
