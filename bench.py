@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=10000)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--e2e-streams", type=int, default=3, help="compute streams (and buffer sets) of the e2e loop")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the float-row precision sub-run and the request-latency burst")
     ap.add_argument("--profile", action="store_true", help="short run for a profiler capture")
@@ -377,7 +378,7 @@ def main():
     # taking the steps in turn and NPIPE buffer sets, and a download stream, so one
     # step's copies overlap its neighbours' searches and the tail of one search (its
     # last, longest queries) overlaps the next searches' start.
-    NPIPE = 3
+    NPIPE = args.e2e_streams
     _, hs, hrr, hbeam = form_of[head]
     h_q = torch.from_numpy(q).pin_memory()
     s_comp = [torch.cuda.Stream() for _ in range(NPIPE)]

@@ -118,7 +118,10 @@ vann_status vann_load_graph(vann_index* index, const char* path, uint64_t n, uin
 vann_status vann_save_graph(vann_index* index, const char* path);
 
 /* Host-array graph upload / download (test and interop path).  consistent=1
- * asserts that every list came from RobustPrune with this index's alpha. */
+ * asserts that every list came from RobustPrune with this index's alpha, as a set:
+ * later batches then re-prune only the nodes that receive new edges (the reference
+ * re-prunes every node, which for such a list gives back the same set in RobustPrune
+ * order; a list held in another order keeps that order until it is touched). */
 vann_status vann_set_graph(vann_index* index, const float* h_vecs, const uint32_t* h_deg,
                            const uint32_t* h_adj, uint64_t n, uint32_t entry, uint32_t consistent);
 vann_status vann_get_graph(vann_index* index, float* h_vecs, uint32_t* h_deg, uint32_t* h_adj);

@@ -65,6 +65,43 @@ def test_insert_matches_reference_patch(oracle, vann_mod):
     assert _rows_equal(gdeg, gadj, g2.deg, g2.adj) == []
 
 
+@pytest.mark.parametrize("stores", [("f32",), ("f32", "u8")], ids=["cuda_cores", "tensor_cores"])
+def test_insert_over_lists_out_of_order(oracle, vann_mod, stores):
+    """The reverse re-prune merges a node's new sources into its list when the list is in
+    RobustPrune order (nondecreasing distance) and sorts the candidates otherwise.  A
+    graph set from outside with every other list reversed takes both paths in one insert
+    batch.  Every row the batch touches (the new rows and the targets of their edges)
+    must equal the oracle's.  The oracle re-prunes every node, as the reference does, so
+    it also puts the untouched reversed lists back in order; the engine, told the lists
+    are consistent, re-prunes only the targets and leaves the other rows as they were."""
+    import torch
+
+    n0, n1, R, L = 3000, 300, 32, 64
+    base = workload.mixture(n0 + n1, 128, 30, seed=36)
+    og, entry = oracle.build_index(base[:n0], R=R, L=L, alpha=1.2, seed=6, skip_mode=2)
+    deg = np.zeros(n0 + n1, np.uint32)
+    adj = np.zeros((n0 + n1, R), np.uint32)
+    deg[:n0] = og.deg
+    for i in range(n0):
+        row = og.adj[i, :og.deg[i]]
+        adj[i, :og.deg[i]] = row[::-1] if i % 2 == 0 else row
+    idx = vann_mod.Index(128, R, L, 1.2, capacity=n0 + n1, stores=stores)
+    idx.set_graph(base[:n0], deg[:n0], adj[:n0], entry, consistent=True)
+    new_ids = idx.insert(torch.from_numpy(base[n0:]).cuda())
+    assert new_ids.cpu().tolist() == list(range(n0, n0 + n1))
+    g2 = oracle.Graph(base, deg.copy(), adj.copy())
+    assert g2.vamana_batch(n0, n1, L, 1.2, entry, skip_mode=0) == 0
+    _, gdeg, gadj = idx.get_graph()
+    live = np.arange(R)[None, :] < g2.deg[n0:, None]
+    touched = np.zeros(n0 + n1, bool)
+    touched[n0:] = True
+    touched[np.unique(g2.adj[n0:][live])] = True
+    want_deg = np.where(touched, g2.deg, deg)
+    want_adj = np.where(touched[:, None], g2.adj, adj)
+    assert _rows_equal(gdeg, gadj, want_deg, want_adj) == []
+    assert 0 < touched[:n0].sum() < n0  # both kinds of old rows occur
+
+
 def test_delete_consolidate_and_reuse(oracle, vann_mod):
     import torch
 
