@@ -580,9 +580,10 @@ def oracle_counts(idx, q, L, sample):
 def precision_subrun(torch, vann, dev, steps, warm, n=1_000_000, nq=10_000, D=96):
     """The reduced-precision configuration's recipe at a size that fits the default run:
     n x 96 float rows from 2,000 unit-norm centres, sigma 0.05 (the 5M x 96 workload of
-    `--config precision`, a fifth of its rows), nq queries.  FP32, BF16+rerank and
-    FP8-E4M3 (per-row scale)+rerank traversal at L in {64, 128}: recall@10, QPS, and the
-    traversal and returned distance errors against FP64."""
+    `--config precision`, a fifth of its rows), nq queries.  FP32, BF16+rerank,
+    FP8-E4M3 (per-row scale)+rerank and uint8 (scalar quantization on the grid fitted
+    to the rows)+rerank traversal at L in {64, 128}: recall@10, QPS, and the traversal
+    and returned distance errors against FP64."""
     from vann import workload
 
     base = workload.mixture(n, D, 2000, seed=11, sigma=0.05, integer=False, unit_norm=True)
@@ -590,7 +591,7 @@ def precision_subrun(torch, vann, dev, steps, warm, n=1_000_000, nq=10_000, D=96
     base_d = torch.from_numpy(base).to(dev)
     q_d = torch.from_numpy(q).to(dev)
     del base
-    idx = vann.Index(D, R, L_BUILD, ALPHA, capacity=n, stores=("f32", "bf16", "fp8"))
+    idx = vann.Index(D, R, L_BUILD, ALPHA, capacity=n, stores=("f32", "bf16", "fp8", "u8"))
     t0 = time.time()
     idx.build(base_d, batch=BATCH, seed=2024)
     torch.cuda.synchronize()
@@ -605,7 +606,7 @@ def precision_subrun(torch, vann, dev, steps, warm, n=1_000_000, nq=10_000, D=96
 
     res = {}
     for L in (64, 128):
-        for store, rr in (("f32", False), ("bf16", True), ("fp8", True)):
+        for store, rr in (("f32", False), ("bf16", True), ("fp8", True), ("u8", True)):
             name = f"{store}{'+rerank' if rr else ''}@L{L}"
             idx.autotune(q_d, k=K, L=L, store=store, rerank=rr)
             ids, d = idx.search(q_d, k=K, L=L, store=store, rerank=rr)
@@ -622,7 +623,7 @@ def precision_subrun(torch, vann, dev, steps, warm, n=1_000_000, nq=10_000, D=96
             res[name] = ent
     for L in (64, 128):
         f = res[f"f32@L{L}"]
-        for s in ("bf16+rerank", "fp8+rerank"):
+        for s in ("bf16+rerank", "fp8+rerank", "u8+rerank"):
             e = res[f"{s}@L{L}"]
             e["recall_loss_vs_f32"] = round(f["recall@10"] - e["recall@10"], 4)
             e["speedup_vs_f32"] = round(e["qps"] / f["qps"], 3)
@@ -870,7 +871,7 @@ def main_precision():
     base_d = torch.from_numpy(base).to(dev)
     q_d = torch.from_numpy(q).to(dev)
     del base
-    idx = vann.Index(D, R, L_BUILD, ALPHA, capacity=n, stores=("f32", "bf16", "fp8"))
+    idx = vann.Index(D, R, L_BUILD, ALPHA, capacity=n, stores=("f32", "bf16", "fp8", "u8"))
     t0 = time.time()
     idx.build(base_d, batch=BATCH, seed=2024)
     torch.cuda.synchronize()
@@ -885,7 +886,7 @@ def main_precision():
 
     res = {}
     for L in (64, 128):
-        for store, rr in (("f32", False), ("bf16", True), ("fp8", True)):
+        for store, rr in (("f32", False), ("bf16", True), ("fp8", True), ("u8", True)):
             name = f"{store}{'+rerank' if rr else ''}@L{L}"
             idx.autotune(q_d, k=K, L=L, store=store, rerank=rr)
             ids, d = idx.search(q_d, k=K, L=L, store=store, rerank=rr)
@@ -903,7 +904,7 @@ def main_precision():
             res[name] = ent
     for L in (64, 128):
         f = res[f"f32@L{L}"]["recall@10"]
-        for s in ("bf16+rerank", "fp8+rerank"):
+        for s in ("bf16+rerank", "fp8+rerank", "u8+rerank"):
             res[f"{s}@L{L}"]["recall_loss_vs_f32"] = round(f - res[f"{s}@L{L}"]["recall@10"], 4)
     line = {"metric": "reduced precision on 5Mx96 float: recall@10, QPS and distance error vs FP64",
             "config": {"workload": f"{n}x{D} float32, 2000 unit-norm centres, sigma 0.05; {nq} queries; "

@@ -86,8 +86,15 @@ __device__ void fp8_row(const float* src, uint8_t* d, float2* scale, const float
     if (lane == 0) *scale = make_float2(sc, sc * sc * cc);
 }
 
-__global__ void convert_kernel(const float* src, void* dst, float2* scale, const float* center, uint64_t rows,
-                               uint32_t D, int store, uint32_t* inexact) {
+// uint8 code of value x: on the identity grid (lo == nullptr) the value itself,
+// rounded and clamped; on a fitted grid round((x - lo[i]) * inv), clamped.
+__device__ __forceinline__ float u8_code(float x, const float* lo, float inv, uint32_t i) {
+    const float v = lo != nullptr ? rintf((x - lo[i]) * inv) : rintf(x);
+    return fminf(fmaxf(v, 0.f), 255.f);
+}
+
+__global__ void convert_kernel(const float* src, void* dst, float2* scale, const float* center, float inv,
+                               uint64_t rows, uint32_t D, int store, uint32_t* inexact) {
     uint64_t r    = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
     uint32_t lane = threadIdx.x & 31u;
     if (r >= rows) return;
@@ -99,28 +106,29 @@ __global__ void convert_kernel(const float* src, void* dst, float2* scale, const
         fp8_row(s, static_cast<uint8_t*>(dst) + r * D, scale + r, center, D, lane);
     } else if (store == 3) {
         uint8_t* d   = static_cast<uint8_t*>(dst) + r * D;
-        bool     off = false;
+        bool     off = center != nullptr;  // a fitted grid is approximate
         for (uint32_t i = lane; i < D; i += 32) {
-            float v = rintf(s[i]);
-            v       = fminf(fmaxf(v, 0.f), 255.f);
-            d[i]    = (uint8_t)v;
+            const float v = u8_code(s[i], center, inv, i);
+            d[i]          = (uint8_t)v;
             off |= !(v == s[i]);
         }
         if (__any_sync(0xffffffffu, off) && lane == 0) atomicOr(inexact, 1u);
     }
 }
 
-cudaError_t launch_convert(const float* src, void* dst, float2* scale, const float* center, uint64_t rows,
-                           uint32_t D, int store, uint32_t* inexact, cudaStream_t st) {
+cudaError_t launch_convert(const float* src, void* dst, float2* scale, const float* center, float inv,
+                           uint64_t rows, uint32_t D, int store, uint32_t* inexact, cudaStream_t st) {
     if (rows == 0) return cudaSuccess;
-    convert_kernel<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(src, dst, scale, center, rows, D, store, inexact);
+    convert_kernel<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(src, dst, scale, center, inv, rows, D, store,
+                                                               inexact);
     return cudaGetLastError();
 }
 
 // Same conversion for rows scattered over an id list (inserts into reused ids):
 // one warp per listed row, the row's traversal copy rewritten from its FP32 row.
 __global__ void convert_ids_kernel(const float* vecs, const uint32_t* ids, uint64_t n, void* dst,
-                                   float2* scale, const float* center, uint32_t D, int store, uint32_t* inexact) {
+                                   float2* scale, const float* center, float inv, uint32_t D, int store,
+                                   uint32_t* inexact) {
     uint64_t i    = blockIdx.x * (uint64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
     uint32_t lane = threadIdx.x & 31u;
     if (i >= n) return;
@@ -133,9 +141,9 @@ __global__ void convert_ids_kernel(const float* vecs, const uint32_t* ids, uint6
         fp8_row(s, static_cast<uint8_t*>(dst) + r * D, scale + r, center, D, lane);
     } else if (store == 3) {
         uint8_t* d   = static_cast<uint8_t*>(dst) + r * D;
-        bool     off = false;
+        bool     off = center != nullptr;
         for (uint32_t k = lane; k < D; k += 32) {
-            const float v = fminf(fmaxf(rintf(s[k]), 0.f), 255.f);
+            const float v = u8_code(s[k], center, inv, k);
             d[k]          = (uint8_t)v;
             off |= !(v == s[k]);
         }
@@ -143,11 +151,91 @@ __global__ void convert_ids_kernel(const float* vecs, const uint32_t* ids, uint6
     }
 }
 cudaError_t launch_convert_ids(const float* vecs, const uint32_t* ids, uint64_t n, void* dst, float2* scale,
-                               const float* center,
-                               uint32_t D, int store, uint32_t* inexact, cudaStream_t st) {
+                               const float* center, float inv, uint32_t D, int store, uint32_t* inexact,
+                               cudaStream_t st) {
     if (n == 0) return cudaSuccess;
-    convert_ids_kernel<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(vecs, ids, n, dst, scale, center, D, store,
+    convert_ids_kernel<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(vecs, ids, n, dst, scale, center, inv, D, store,
                                                                 inexact);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- uint8 grid
+// The uint8 copy's grid, fitted to rows 0 .. n-1.  When every value is an integer
+// in [0, 255] the grid is the identity and the copy is exact.  Otherwise every
+// dimension gets its own offset lo[i] (the column minimum) and all share one
+// scale s = max_i (max_i - lo[i]) / 255, so a squared distance on the codes is the
+// squared distance on the rows divided by s^2 (up to rounding): traversal orders
+// them alike, and s^2 brings the code distance back to the rows' units.
+// ws (u8_grid_ws_bytes): per column the ordered bits of the minimum and maximum,
+// then the off-grid flag.  grid out: {affine (0 / 1 as float), s, 1 / s}.
+
+// order-preserving map of a float onto uint32 (ascending floats -> ascending words)
+__device__ __forceinline__ uint32_t ord_bits(float x) {
+    const uint32_t b = __float_as_uint(x);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float ord_float(uint32_t w) {
+    return __uint_as_float((w & 0x80000000u) ? (w & 0x7fffffffu) : ~w);
+}
+
+__global__ void u8_minmax_kernel(const float* vecs, uint64_t n, uint32_t D, uint32_t* mn, uint32_t* mx,
+                                 uint32_t* off) {
+    const uint32_t d = threadIdx.x + blockIdx.y * blockDim.x;
+    if (d >= D) return;
+    const uint64_t r0 = blockIdx.x * (uint64_t)1024;
+    const uint64_t r1 = n < r0 + 1024 ? n : r0 + 1024;
+    uint32_t       lo = 0xffffffffu, hi = 0u;
+    bool           bad = false;
+    for (uint64_t r = r0; r < r1; ++r) {
+        const float x = vecs[r * D + d];
+        lo            = min(lo, ord_bits(x));
+        hi            = max(hi, ord_bits(x));
+        bad |= !(x >= 0.f && x <= 255.f && rintf(x) == x);
+    }
+    atomicMin(mn + d, lo);
+    atomicMax(mx + d, hi);
+    if (bad) atomicOr(off, 1u);
+}
+
+// one block: lo[] and grid[] from the column bounds
+__global__ void u8_grid_kernel(const uint32_t* mn, const uint32_t* mx, const uint32_t* off, uint32_t D,
+                               float* lo, float* grid) {
+    __shared__ float red[32];
+    const bool affine = *off != 0u;
+    float      range  = 0.f;
+    for (uint32_t d = threadIdx.x; d < D; d += blockDim.x) {
+        const float a = ord_float(mn[d]);
+        lo[d]         = affine ? a : 0.f;
+        range         = fmaxf(range, ord_float(mx[d]) - a);
+    }
+    for (int o = 16; o; o >>= 1) range = fmaxf(range, __shfl_xor_sync(0xffffffffu, range, o));
+    if ((threadIdx.x & 31u) == 0) red[threadIdx.x >> 5] = range;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (uint32_t w = 1; w < blockDim.x / 32; ++w) range = fmaxf(range, red[w]);
+        const float s = affine && range > 0.f ? range / 255.f : 1.f;
+        grid[0]       = affine ? 1.f : 0.f;
+        grid[1]       = s;
+        grid[2]       = 1.f / s;
+    }
+}
+
+size_t u8_grid_ws_bytes(uint32_t D) { return sizeof(uint32_t) * (2ull * D + 1); }
+
+cudaError_t launch_u8_grid(const float* vecs, uint64_t n, uint32_t D, void* ws, float* lo, float* grid,
+                           cudaStream_t st) {
+    auto*       mn  = static_cast<uint32_t*>(ws);
+    uint32_t*   mx  = mn + D;
+    uint32_t*   off = mx + D;
+    cudaError_t e   = cudaMemsetAsync(mn, 0xff, sizeof(uint32_t) * D, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(mx, 0, sizeof(uint32_t) * (D + 1), st);
+    if (e != cudaSuccess) return e;
+    if (n > 0) {
+        const dim3 g((unsigned)((n + 1023) / 1024), (D + 127) / 128);
+        u8_minmax_kernel<<<g, 128, 0, st>>>(vecs, n, D, mn, mx, off);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    u8_grid_kernel<<<1, 256, 0, st>>>(mn, mx, off, D, lo, grid);
     return cudaGetLastError();
 }
 

@@ -216,6 +216,10 @@ struct vann_index {
     void*     store[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // by vann_store
     float2*   fp8_scale = nullptr;  // per row (scale, scale^2 |codes|^2)
     float*    fp8_center = nullptr; // per dimension: the FP8 codes encode row - center
+    float*    u8_lo = nullptr;      // uint8 copy: per-dimension offsets of its grid
+    float*    u8_grid = nullptr;    // uint8 copy: {affine flag, scale, 1 / scale}
+    bool      u8_affine = false;    // host copy of the grid: fitted (approximate) or identity
+    float     u8_s = 1.f, u8_inv = 1.f;
     float*    pq_cb = nullptr;      // PQ copy: [D / 8][256][8] centroids
     float*    pq_cnorm = nullptr;   // PQ copy: [D / 8] largest centroid norm per subspace
     uint32_t* deg  = nullptr;
@@ -259,6 +263,8 @@ struct vann_index {
         for (void* s : store) cudaFree(s);
         cudaFree(fp8_scale);
         cudaFree(fp8_center);
+        cudaFree(u8_lo);
+        cudaFree(u8_grid);
         cudaFree(pq_cb);
         cudaFree(pq_cnorm);
         cudaFree(deg);
@@ -344,9 +350,17 @@ struct vann_index {
         return u8_state == 1;
     }
 
+    // the centre / offsets argument of the conversion kernels for traversal copy s
+    const float* copy_center(int s) const {
+        if (s == 2) return fp8_center;
+        if (s == 3 && u8_affine) return u8_lo;
+        return nullptr;
+    }
+
     // rows [first, first + rows) -> traversal copies; rows from 0 replace every
     // row, so the uint8 exactness flag starts over and the FP8 centre (the rows'
-    // column means, fixed until the rows are replaced again) is recomputed
+    // column means) and the uint8 grid, both fixed until the rows are replaced
+    // again, are recomputed
     void convert_rows(uint64_t first, uint64_t rows, cudaStream_t st) {
         u8_state = -1;
         if (first == 0) VCHECK(cudaMemsetAsync(u8_inexact(), 0, sizeof(uint32_t), st));
@@ -354,12 +368,24 @@ struct vann_index {
             medoid_ws.ensure(vann::medoid_ws_bytes(p.dim));
             VCHECK(vann::launch_col_mean(vecs, rows, p.dim, medoid_ws.p, fp8_center, st));
         }
+        if (first == 0 && store[3] && rows > 0) {
+            // the grid: identity for rows of integers in [0, 255], else fitted; the
+            // host keeps a copy for the search launches
+            medoid_ws.ensure(std::max(vann::medoid_ws_bytes(p.dim), vann::u8_grid_ws_bytes(p.dim)));
+            VCHECK(vann::launch_u8_grid(vecs, rows, p.dim, medoid_ws.p, u8_lo, u8_grid, st));
+            float g[3] = {0.f, 1.f, 1.f};
+            VCHECK(cudaMemcpyAsync(g, u8_grid, sizeof(g), cudaMemcpyDeviceToHost, st));
+            VCHECK(cudaStreamSynchronize(st));
+            u8_affine = g[0] != 0.f;
+            u8_s      = g[1];
+            u8_inv    = g[2];
+        }
         for (int s = 1; s < 4; ++s) {
             if (!store[s]) continue;
             size_t esz = s == 1 ? 2 : 1;
             void*  dst = static_cast<char*>(store[s]) + first * p.dim * esz;
             VCHECK(vann::launch_convert(vecs + first * p.dim, dst, s == 2 ? fp8_scale + first : nullptr,
-                                        s == 2 ? fp8_center : nullptr, rows, p.dim, s, u8_inexact(), st));
+                                        copy_center(s), u8_inv, rows, p.dim, s, u8_inexact(), st));
         }
         if (store[4] && rows > 0) {
             // PQ: the codebook is trained on the rows that replace every row, then fixed
@@ -699,7 +725,11 @@ vann_status vann_create(const vann_params* params, vann_index** out) {
                 h->alloc((void**)&h->fp8_scale, sizeof(float2) * C);
                 h->alloc((void**)&h->fp8_center, sizeof(float) * p.dim);
             }
-            if (p.stores & (1u << VANN_STORE_U8)) h->alloc(&h->store[3], 1ull * C * p.dim);
+            if (p.stores & (1u << VANN_STORE_U8)) {
+                h->alloc(&h->store[3], 1ull * C * p.dim);
+                h->alloc((void**)&h->u8_lo, sizeof(float) * p.dim);
+                h->alloc((void**)&h->u8_grid, sizeof(float) * 4);
+            }
             if (p.stores & (1u << VANN_STORE_PQ)) {
                 h->alloc(&h->store[4], 1ull * C * (p.dim / vann::kPqSub));
                 h->alloc((void**)&h->pq_cb, sizeof(float) * (size_t)p.dim * vann::kPqK);
@@ -1039,7 +1069,11 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
         a.beam  = vann_index::beam_of(*sp);
         a.store = h->store[sp->store];
         a.scale = h->fp8_scale;
-        a.center = sp->store == VANN_STORE_FP8 ? h->fp8_center : nullptr;
+        a.center = sp->store == VANN_STORE_FP8 || sp->store == VANN_STORE_U8 ? h->copy_center(sp->store) : nullptr;
+        if (sp->store == VANN_STORE_U8 && h->u8_affine) {  // code distances, scaled back on output
+            a.u8_inv    = h->u8_inv;
+            a.out_scale = h->u8_s * h->u8_s;
+        }
         a.pq_cb = h->pq_cb;
         a.pq_cnorm = h->pq_cnorm;
         a.vecs_f32 = h->vecs;
@@ -1250,7 +1284,7 @@ vann_status vann_insert(vann_index* h, const float* d_vecs, uint64_t n, uint32_t
             for (int s = 1; s < 4; ++s)  // reused ids are scattered: convert by id list
                 if (h->store[s])
                     VCHECK(vann::launch_convert_ids(h->vecs, h->nodes.as<uint32_t>(), n, h->store[s],
-                                                    s == 2 ? h->fp8_scale : nullptr, s == 2 ? h->fp8_center : nullptr,
+                                                    s == 2 ? h->fp8_scale : nullptr, h->copy_center(s), h->u8_inv,
                                                     D, s, h->u8_inexact(), st));
             if (h->store[4])
                 VCHECK(vann::launch_pq_encode(h->vecs, 0, n, h->nodes.as<uint32_t>(), D, h->pq_cb,

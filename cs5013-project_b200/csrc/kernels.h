@@ -14,7 +14,11 @@ void set_last_error(const char* msg);
 struct SearchArgs {
     const void*     store;     // traversal copy (F32 / BF16 / FP8 / U8 rows)
     const float2*   scale;     // FP8 copy: per row (scale, scale^2 * |codes|^2)
-    const float*    center;    // FP8 copy: per-dimension centre the codes are relative to
+    const float*    center;    // FP8 copy: per-dimension centre the codes are relative to;
+                               // uint8 copy on a fitted grid: its per-dimension offsets
+    float           u8_inv = 1.f;     // uint8 copy on a fitted grid: 1 / its scale
+    float           out_scale = 1.f;  // factor on returned traversal distances (scale^2 of a
+                                      // fitted uint8 grid; 1 otherwise)
     const float*    pq_cb;     // PQ copy: [D / 8][256][8] centroids
     const float*    pq_cnorm;  // PQ copy: [D / 8] largest centroid norm per subspace
     const float*    vecs_f32;  // exact rows (rerank)
@@ -127,12 +131,20 @@ cudaError_t launch_random_graph(uint32_t* deg, uint32_t* adj, uint32_t* adj_h, u
 cudaError_t launch_hash_rows(const uint32_t* adj, uint32_t* adj_h, uint64_t n, uint32_t R,
                              cudaStream_t st);
 // inexact: set non-zero when a uint8 code is not exactly its FP32 value
-// FP8 only: the codes encode row - center[] with scale[row] = (s, s^2 * |codes|^2),
-// s = amax / 448 of the centred row
-cudaError_t launch_convert(const float* src, void* dst, float2* scale, const float* center, uint64_t rows,
-                           uint32_t D, int store, uint32_t* inexact, cudaStream_t st);
+// FP8: the codes encode row - center[] with scale[row] = (s, s^2 * |codes|^2),
+// s = amax / 448 of the centred row.  uint8: center = the fitted grid's offsets and
+// inv its 1 / scale (launch_u8_grid), or nullptr for the identity grid.
+cudaError_t launch_convert(const float* src, void* dst, float2* scale, const float* center, float inv,
+                           uint64_t rows, uint32_t D, int store, uint32_t* inexact, cudaStream_t st);
 cudaError_t launch_convert_ids(const float* vecs, const uint32_t* ids, uint64_t n, void* dst, float2* scale,
-                               const float* center, uint32_t D, int store, uint32_t* inexact, cudaStream_t st);
+                               const float* center, float inv, uint32_t D, int store, uint32_t* inexact,
+                               cudaStream_t st);
+// The uint8 copy's grid fitted to rows 0 .. n-1: lo[D] offsets and grid[3] =
+// {affine flag, scale, 1 / scale}; the identity (lo 0, scale 1, flag 0) when every
+// value is an integer in [0, 255].  ws: u8_grid_ws_bytes(D).
+size_t      u8_grid_ws_bytes(uint32_t D);
+cudaError_t launch_u8_grid(const float* vecs, uint64_t n, uint32_t D, void* ws, float* lo, float* grid,
+                           cudaStream_t st);
 // float bits of each column's largest magnitude over rows 0 .. n-1
 cudaError_t launch_col_bounds(const float* vecs, uint64_t n, uint32_t D, uint32_t* bound, cudaStream_t st);
 // PQ codebook (pq.cu): cb [D / 8][256][8] centroids trained on rows 0 .. n-1, cnorm [D / 8]

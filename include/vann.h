@@ -43,7 +43,13 @@ typedef enum {
     VANN_STORE_F32  = 0,
     VANN_STORE_BF16 = 1, /* round-to-nearest-even bf16, FP32 accumulation */
     VANN_STORE_FP8  = 2, /* e4m3 with one FP32 scale per vector (amax / 448) */
-    VANN_STORE_U8   = 3, /* uint8 codes; exact for integer data in [0, 255] */
+    VANN_STORE_U8   = 3, /* uint8 codes on a grid fitted to the rows that fill the
+                            index (build / set / load): the identity, so the copy is
+                            exact, when every value is an integer in [0, 255]; else
+                            one offset per dimension (its minimum) and one scale
+                            (the largest range / 255), queries rounded onto the same
+                            grid, returned distances scaled back (approximate: meant
+                            for rerank = 1).  Later inserts keep the grid. */
     VANN_STORE_PQ   = 4  /* product-quantized codes: one byte per 8 dimensions (256
                             k-means centroids per subspace), distances from a per-query
                             table; approximate, meant for rerank = 1; dim a multiple

@@ -1,0 +1,130 @@
+"""The uint8 traversal copy on float rows: scalar quantization onto a fitted grid.
+
+Rows that are not all integers in [0, 255] get a grid with one offset per dimension
+(the column minimum) and one scale s = max over dimensions of (max - min) / 255.
+Codes are round((x - lo) / s), clamped to [0, 255]; a query is mapped onto the same
+grid and rounded, and the search runs the exact dp4a path on the codes.  Returned
+traversal distances are the code distances times s^2, so they are restated here bit
+for bit in numpy (FP32 arithmetic, as the kernels do it).  With rerank the returned
+distances are exact FP32 and recall matches the FP32 form's.
+"""
+import numpy as np
+import pytest
+
+from vann import workload
+
+pytestmark = pytest.mark.gpu
+
+
+def _grid(rows):
+    """The grid the library fits to `rows`: offsets, scale, 1 / scale (all FP32)."""
+    rows = rows.astype(np.float32)
+    lo = rows.min(0)
+    rng = (rows.max(0) - lo).max()
+    s = np.float32(rng) / np.float32(255.0) if rng > 0 else np.float32(1.0)
+    return lo, np.float32(s), np.float32(1.0) / np.float32(s)
+
+
+def _codes(x, lo, inv):
+    return np.clip(np.rint((x.astype(np.float32) - lo) * inv), 0, 255).astype(np.int64)
+
+
+def _code_dists(q, base, ids, lo, s, inv):
+    """s^2 * squared code distance of every returned id, as the kernel forms it."""
+    qc = _codes(q, lo, inv)
+    bc = _codes(base, lo, inv)
+    out = np.empty(ids.shape, np.float32)
+    s2 = np.float32(s) * np.float32(s)
+    for i in range(ids.shape[0]):
+        dd = ((bc[ids[i]] - qc[i][None, :]) ** 2).sum(-1)
+        out[i] = dd.astype(np.float32) * s2
+    return out
+
+
+def _fixture(n=6000, D=96, seed=81):
+    base = workload.mixture(n, D, 30, seed=seed, sigma=0.05, integer=False, unit_norm=True)
+    q = workload.mixture(200, D, 30, seed=seed + 1, sigma=0.05, integer=False, unit_norm=True)
+    return base, q
+
+
+def test_fitted_grid_traversal_distances_bit_exact(vann_mod):
+    import torch
+
+    base, q = _fixture()
+    n, D = base.shape
+    idx = vann_mod.Index(D, 32, 48, 1.2, capacity=n, stores=("f32", "u8"))
+    idx.build(torch.from_numpy(base).cuda(), batch=2000, seed=5)
+    assert idx.info()["entry"] < n
+    lo, s, inv = _grid(base)
+    qd = torch.from_numpy(q).cuda()
+    for L in (32, 48):
+        ids, d = idx.search(qd, k=10, L=L, store="u8", rerank=False)
+        gi = ids.cpu().numpy().view(np.uint32)
+        gd = d.cpu().numpy()
+        assert (gi < n).all()
+        assert np.array_equal(gd, _code_dists(q, base, gi.astype(np.int64), lo, s, inv))
+        assert (np.diff(gd, axis=1) >= 0).all()
+
+
+def test_fitted_grid_rerank_recall_and_exact_distances(oracle, vann_mod):
+    import torch
+
+    base, q = _fixture(n=20000, seed=83)
+    n, D = base.shape
+    idx = vann_mod.Index(D, 32, 64, 1.2, capacity=n, stores=("f32", "u8"))
+    idx.build(torch.from_numpy(base).cuda(), batch=5000, seed=6)
+    qd = torch.from_numpy(q).cuda()
+    truth, _ = oracle.bruteforce_knn(base, q, 10)
+    ids32, _ = idx.search(qd, k=10, L=64)
+    r32 = oracle.recall_at_k(ids32.cpu().numpy(), truth, 10)
+    assert r32 >= 0.95
+    ids, d = idx.search(qd, k=10, L=64, store="u8", rerank=True)
+    gi = ids.cpu().numpy()
+    assert oracle.recall_at_k(gi, truth, 10) >= r32 - 0.01
+    ex = ((base[gi].astype(np.float64) - q[:, None, :].astype(np.float64)) ** 2).sum(-1)
+    assert np.allclose(d.cpu().numpy(), ex, rtol=1e-5, atol=1e-7)
+    # traversal distances against FP64: the grid's step is ~0.4% of the data's range;
+    # on this recipe the error stays within a few percent of the distance
+    ids2, d2 = idx.search(qd, k=10, L=64, store="u8", rerank=False)
+    g2 = ids2.cpu().numpy()
+    ex2 = ((base[g2].astype(np.float64) - q[:, None, :].astype(np.float64)) ** 2).sum(-1)
+    rel = np.abs(d2.cpu().numpy() - ex2) / np.maximum(ex2, 1e-30)
+    assert rel.mean() < 5e-3 and rel.max() < 0.05, (rel.mean(), rel.max())
+
+
+def test_grid_fixed_for_later_inserts(vann_mod):
+    """Rows inserted after the build are coded on the build's grid (no refit), values
+    beyond its range clamped to the end codes."""
+    import torch
+
+    base, q = _fixture(n=5000, seed=85)
+    n, D = base.shape
+    first = 4000
+    extra = base[first:].copy()
+    extra[:50] *= 1.5  # some rows beyond the fitted range
+    rows = np.concatenate([base[:first], extra])
+    idx = vann_mod.Index(D, 32, 48, 1.2, capacity=n, stores=("f32", "u8"))
+    idx.build(torch.from_numpy(rows[:first]).cuda(), batch=0, seed=7)
+    idx.insert(torch.from_numpy(rows[first:]).cuda())
+    idx.sync()
+    lo, s, inv = _grid(rows[:first])
+    ids, d = idx.search(torch.from_numpy(q).cuda(), k=10, L=48, store="u8", rerank=False)
+    gi = ids.cpu().numpy().view(np.uint32).astype(np.int64)
+    assert np.array_equal(d.cpu().numpy(), _code_dists(q, rows, gi, lo, s, inv))
+    assert (gi >= first).any()  # inserted rows are found
+
+
+def test_integer_rows_keep_the_identity_grid(oracle, vann_mod):
+    """Integer rows in [0, 255]: the copy stays exact and distances are the oracle's."""
+    import torch
+
+    base = workload.mixture(3000, 128, 20, seed=87)
+    q = workload.mixture(64, 128, 20, seed=88)
+    g, entry = oracle.build_index(base, R=32, L=48, alpha=1.2, seed=1)
+    idx = vann_mod.Index(128, 32, 48, 1.2, capacity=3000, stores=("f32", "u8"))
+    idx.set_graph(base, g.deg, g.adj, entry, consistent=True)
+    ids, d = idx.search(torch.from_numpy(q).cuda(), k=10, L=48, store="u8")
+    st, oids, od, _, _ = g.search(q, 48, 10, entry)
+    assert st == 0
+    assert np.array_equal(ids.cpu().numpy().view(np.uint32), oids)
+    assert np.array_equal(d.cpu().numpy(), od)
