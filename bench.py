@@ -882,8 +882,10 @@ def main_churn():
 
 def main_precision():
     """Reduced precision on float data: 5M x 96 from a 2,000-cluster mixture with unit-norm
-    centres and sigma 0.05; FP32, BF16+rerank and FP8-E4M3 (per-row scale)+rerank traversal;
-    recall@10 at L in {64, 128}, QPS, and the traversal distance error against FP64."""
+    centres and sigma 0.05; FP32, BF16+rerank, FP8-E4M3 (per-row scale)+rerank and uint8
+    (scalar quantization on the fitted grid)+rerank traversal; recall@10 at L in {64, 128},
+    QPS, the traversal distance error against FP64, and each form at its own smallest L
+    with recall@10 >= 0.95.  --only FORM@L (e.g. u8+rerank@80) times one form at one L."""
     args = parse()
     import torch
 
@@ -912,13 +914,20 @@ def main_precision():
         return ((d.double() - exact).abs() / exact.clamp(min=1e-30))[ids >= 0]
 
     res = {}
-    for L in (64, 128):
-        for store, rr in (("f32", False), ("bf16", True), ("fp8", True), ("u8", True)):
+    forms, Ls = (("f32", False), ("bf16", True), ("fp8", True), ("u8", True)), (64, 128)
+    steps, warm = (3, 1) if args.profile else (args.steps, args.warmup)
+    if args.only:  # one form at one L, default launch variant (a profiler capture of one instantiation)
+        oname, oL = args.only.split("@")
+        forms = tuple(f for f in forms if f"{f[0]}{'+rerank' if f[1] else ''}" == oname)
+        Ls = (int(oL),)
+    for L in Ls:
+        for store, rr in forms:
             name = f"{store}{'+rerank' if rr else ''}@L{L}"
-            idx.autotune(q_d, k=K, L=L, store=store, rerank=rr)
+            if not args.only:
+                idx.autotune(q_d, k=K, L=L, store=store, rerank=rr)
             ids, d = idx.search(q_d, k=K, L=L, store=store, rerank=rr)
             t = time_steps(torch, lambda s=store, rr=rr, L=L: idx.search(q_d, k=K, L=L, store=s, rerank=rr),
-                           args.steps, args.warmup, flush)
+                           steps, warm, flush)
             ent = {"recall@10": round(recall(torch, ids, gt), 4),
                    "qps": round(nq / (statistics.mean(t) / 1e3), 1),
                    "returned_max_rel_err": float(rel_err(ids, d).max())}
@@ -929,12 +938,17 @@ def main_precision():
                 ent["traversal_mean_rel_err"] = float(e2.mean())
                 ent["recall@10_no_rerank"] = round(recall(torch, ids2, gt), 4)
             res[name] = ent
-    for L in (64, 128):
+    for L in Ls:
+        if f"f32@L{L}" not in res:
+            continue
         f = res[f"f32@L{L}"]["recall@10"]
         for s in ("bf16+rerank", "fp8+rerank", "u8+rerank"):
-            res[f"{s}@L{L}"]["recall_loss_vs_f32"] = round(f - res[f"{s}@L{L}"]["recall@10"], 4)
-    at_target = precision_operating_points(torch, idx, q_d, gt, (64, 72, 80, 88, 96, 112, 128, 160), args.steps,
-                                           args.warmup, flush, nq)
+            if f"{s}@L{L}" in res:
+                res[f"{s}@L{L}"]["recall_loss_vs_f32"] = round(f - res[f"{s}@L{L}"]["recall@10"], 4)
+    at_target = None
+    if not args.only:
+        at_target = precision_operating_points(torch, idx, q_d, gt, (64, 72, 80, 88, 96, 112, 128, 160),
+                                               args.steps, args.warmup, flush, nq)
     line = {"metric": "reduced precision on 5Mx96 float: recall@10, QPS and distance error vs FP64",
             "config": {"workload": f"{n}x{D} float32, 2000 unit-norm centres, sigma 0.05; {nq} queries; "
                                    f"R={R} L={L_BUILD} alpha={ALPHA}; k={K}", "build_s": round(build_s, 2)},
