@@ -22,7 +22,8 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-ccbin", "g++
          "--expt-relaxed-constexpr", "-Wno-deprecated-gpu-targets"]
 SOURCES = ["search.cu", "search_f32.cu", "search_bf16.cu", "search_fp8.cu", "search_u8.cu", "search_pq.cu", "pq.cu",
            "prune.cu",
-           "prune_tc.cu", "prune_rev.cu", "staged.cu", "formats.cu", "graph_ops.cu", "index.cu", "server.cu"]
+           "prune_tc.cu", "prune_rev.cu", "staged.cu", "formats.cu", "graph_ops.cu", "index.cu", "server.cu",
+           "rerank.cu"]
 HEADERS = ["common.cuh", "kernels.h", "search_impl.cuh", "search_reg.cuh", "search_dispatch.cuh"]
 
 

@@ -183,12 +183,9 @@ struct Query {
 
 // center (scaled stores): the per-dimension centre the row codes are relative to;
 // the query is centred the same way, which leaves every distance unchanged.
-// center (uint8 rows on a fitted grid): the grid's per-dimension offsets, with inv =
-// 1 / its scale; the query is mapped onto the same grid and rounded to its nearest
-// code, clamped to [0, 255], so the exact dp4a path runs on code distances.
 template <typename S, int DC>
 __device__ __forceinline__ void load_query(Query<S, DC>& q, const float* row, uint32_t D, uint32_t lane,
-                                           const float* center = nullptr, float inv = 1.f) {
+                                           const float* center = nullptr) {
     if constexpr (S::kPQ) {  // the PQ query is its distance table (build_pq_lut)
         q.row  = row;
         q.qint = false;
@@ -215,15 +212,6 @@ __device__ __forceinline__ void load_query(Query<S, DC>& q, const float* row, ui
                     x.y -= cz.y;
                     x.z -= cz.z;
                     x.w -= cz.w;
-                }
-            }
-            if constexpr (S::kInt) {
-                if (center != nullptr && valid) {
-                    const float4 lo = __ldg(reinterpret_cast<const float4*>(center + k * S::kElems) + v);
-                    x.x             = fminf(fmaxf(rintf((x.x - lo.x) * inv), 0.f), 255.f);
-                    x.y             = fminf(fmaxf(rintf((x.y - lo.y) * inv), 0.f), 255.f);
-                    x.z             = fminf(fmaxf(rintf((x.z - lo.z) * inv), 0.f), 255.f);
-                    x.w             = fminf(fmaxf(rintf((x.w - lo.w) * inv), 0.f), 255.f);
                 }
             }
             float  e[4] = {x.x, x.y, x.z, x.w};

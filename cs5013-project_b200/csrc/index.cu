@@ -250,6 +250,9 @@ struct vann_index {
     // search order of large batches (distance keys, then the order), one workspace per
     // stream: searches in flight on different streams (the server's slots) never share it
     std::map<cudaStream_t, DevBuf> ord;
+    // per stream, searches over the fitted uint8 grid: the queries on the grid and the
+    // candidate lists of the rerank
+    std::map<cudaStream_t, DevBuf> grid_ws;
     std::vector<void*>             ord_retired;  // outgrown order workspaces, freed at destroy
     DevBuf vis_ids, vis_d, vis_n, nodes, runs, ovf, stage, s2_ids, s2_d, e_keys, e_vals, e_keys2, e_vals2, counts, offsets, cub_tmp,
         medoid_ws, gather, cand, cand_n, list_n, out_tmp;
@@ -274,6 +277,7 @@ struct vann_index {
         cudaFree(counters);
         cudaFree(status);
         for (auto& o : ord) o.second.release();
+        for (auto& o : grid_ws) o.second.release();
         for (void* r : ord_retired) cudaFree(r);
         for (DevBuf* b : {&vis_ids, &vis_d, &vis_n, &nodes, &runs, &ovf, &stage, &s2_ids, &s2_d, &e_keys, &e_vals, &e_keys2, &e_vals2,
                           &counts, &offsets, &cub_tmp, &medoid_ws, &gather, &cand, &cand_n,
@@ -1069,11 +1073,7 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
         a.beam  = vann_index::beam_of(*sp);
         a.store = h->store[sp->store];
         a.scale = h->fp8_scale;
-        a.center = sp->store == VANN_STORE_FP8 || sp->store == VANN_STORE_U8 ? h->copy_center(sp->store) : nullptr;
-        if (sp->store == VANN_STORE_U8 && h->u8_affine) {  // code distances, scaled back on output
-            a.u8_inv    = h->u8_inv;
-            a.out_scale = h->u8_s * h->u8_s;
-        }
+        a.center = sp->store == VANN_STORE_FP8 ? h->fp8_center : nullptr;
         a.pq_cb = h->pq_cb;
         a.pq_cnorm = h->pq_cnorm;
         a.vecs_f32 = h->vecs;
@@ -1105,6 +1105,47 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
         if (a.order == nullptr) VCHECK(cudaMemsetAsync(a.counter, 0, sizeof(uint32_t), S(stream)));
         a.pdl = chain ? 1 : 0;
         a.status = h->status;
+        if (sp->store == VANN_STORE_U8 && h->u8_affine) {
+            // uint8 copy on a fitted grid: the queries rounded onto the grid, the search on
+            // code distances, then the exact FP32 rerank of each list, or the distances
+            // scaled back by s^2 (the queries' order above comes from the FP32 queries)
+            cudaStream_t   st   = S(stream);
+            const uint32_t L    = sp->L;
+            const size_t   qb   = sizeof(float) * nq * h->p.dim;
+            const size_t   cb   = sp->rerank ? (sizeof(uint32_t) + sizeof(float)) * nq * L : 0;
+            DevBuf&        ws   = h->grid_ws[st];
+            if (ws.bytes < qb + cb) {
+                cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+                VCHECK(cudaStreamIsCapturing(st, &cs));
+                VREQUIRE(cs == cudaStreamCaptureStatusNone, VANN_ERR_STATE,
+                         "a search over the fitted uint8 grid needs its workspace before capture: run one "
+                         "search of this size on the stream first");
+                if (ws.p) {  // a captured search may hold the old one: keep it until destroy
+                    h->ord_retired.push_back(ws.p);
+                    ws.p     = nullptr;
+                    ws.bytes = 0;
+                }
+                ws.ensure(qb + cb);
+            }
+            float* qg = ws.as<float>();
+            VCHECK(vann::launch_grid_queries(d_queries, nq, h->p.dim, h->u8_lo, h->u8_inv, qg, st));
+            a.queries = qg;
+            a.rerank  = 0;
+            if (sp->rerank) {
+                uint32_t* cand = reinterpret_cast<uint32_t*>(static_cast<char*>(ws.p) + qb);
+                a.k       = L;
+                a.kq      = nullptr;  // every list whole: the rerank applies k
+                a.out_ids = cand;
+                a.out_d   = reinterpret_cast<float*>(cand + nq * L);
+                VCHECK(vann::launch_search(a, (int)sp->store, h->num_sms, st, h->variant_for(*sp)));
+                VCHECK(vann::launch_rerank(h->vecs, d_queries, nq, h->p.dim, cand, L, h->pending_kq, sp->k, d_ids,
+                                           d_dists, h->num_sms, st));
+            } else {
+                VCHECK(vann::launch_search(a, (int)sp->store, h->num_sms, st, h->variant_for(*sp)));
+                VCHECK(vann::launch_scale(d_dists, nq * sp->k, h->u8_s * h->u8_s, st));
+            }
+            return;
+        }
         VCHECK(vann::launch_search(a, (int)sp->store, h->num_sms, S(stream), h->variant_for(*sp)));
     });
 }

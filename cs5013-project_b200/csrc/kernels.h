@@ -14,11 +14,7 @@ void set_last_error(const char* msg);
 struct SearchArgs {
     const void*     store;     // traversal copy (F32 / BF16 / FP8 / U8 rows)
     const float2*   scale;     // FP8 copy: per row (scale, scale^2 * |codes|^2)
-    const float*    center;    // FP8 copy: per-dimension centre the codes are relative to;
-                               // uint8 copy on a fitted grid: its per-dimension offsets
-    float           u8_inv = 1.f;     // uint8 copy on a fitted grid: 1 / its scale
-    float           out_scale = 1.f;  // factor on returned traversal distances (scale^2 of a
-                                      // fitted uint8 grid; 1 otherwise)
+    const float*    center;    // FP8 copy: per-dimension centre the codes are relative to
     const float*    pq_cb;     // PQ copy: [D / 8][256][8] centroids
     const float*    pq_cnorm;  // PQ copy: [D / 8] largest centroid norm per subspace
     const float*    vecs_f32;  // exact rows (rerank)
@@ -145,6 +141,21 @@ cudaError_t launch_convert_ids(const float* vecs, const uint32_t* ids, uint64_t 
 size_t      u8_grid_ws_bytes(uint32_t D);
 cudaError_t launch_u8_grid(const float* vecs, uint64_t n, uint32_t D, void* ws, float* lo, float* grid,
                            cudaStream_t st);
+
+// Searches over a uint8 copy on a fitted grid (rerank.cu).  The queries are mapped onto
+// the grid first -- round((q - lo) / s) clamped to [0, 255], an integer-valued FP32 copy
+// -- so the search kernels run their exact integer path on code distances; the result
+// is then either reranked from the exact FP32 rows or its distances scaled by s^2.
+cudaError_t launch_grid_queries(const float* q, uint64_t nq, uint32_t D, const float* lo, float inv, float* out,
+                                cudaStream_t st);
+// Exact FP32 rerank of per-query candidate lists: cand [nq][L] in worklist order
+// (kNone past the list's end) -> the k closest by (exact distance, list position),
+// per-query counts kq (or null: k for all); the rerank the search kernels apply
+// in-kernel, as a separate pass.
+cudaError_t launch_rerank(const float* vecs, const float* q, uint64_t nq, uint32_t D, const uint32_t* cand,
+                          uint32_t L, const uint32_t* kq, uint32_t k, uint32_t* out_ids, float* out_d,
+                          int num_sms, cudaStream_t st);
+cudaError_t launch_scale(float* x, uint64_t n, float f, cudaStream_t st);
 // float bits of each column's largest magnitude over rows 0 .. n-1
 cudaError_t launch_col_bounds(const float* vecs, uint64_t n, uint32_t D, uint32_t* bound, cudaStream_t st);
 // PQ codebook (pq.cu): cb [D / 8][256][8] centroids trained on rows 0 .. n-1, cnorm [D / 8]

@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
         const uint32_t kq = a.kq != nullptr ? min(__ldg(a.kq + q), a.k) : a.k;
 
         Query<S, DC> qv;
-        load_query<S, DC>(qv, a.queries + (uint64_t)q * a.D, a.D, lane, a.center, a.u8_inv);
+        load_query<S, DC>(qv, a.queries + (uint64_t)q * a.D, a.D, lane, a.center);
         if constexpr (S::kPQ)
             build_pq_lut<DC>(qv, reinterpret_cast<uint16_t*>(base + lay.lut), a.pq_cb, a.pq_cnorm,
                              a.queries + (uint64_t)q * a.D, a.D, lane);
@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
                     uint64_t o = (uint64_t)q * a.k + t;
                     if (t < n && t < kq) {
                         a.out_ids[o] = wl_id[t] & ~kVisitedBit;
-                        a.out_d[o]   = wl_d[t] * a.out_scale;
+                        a.out_d[o]   = wl_d[t];
                     } else {
                         a.out_ids[o] = kNone;
                         a.out_d[o]   = __int_as_float(0x7f800000);

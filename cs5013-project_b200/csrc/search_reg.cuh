@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
         const uint32_t kq = a.kq != nullptr ? min(__ldg(a.kq + q), a.k) : a.k;
 
         Query<S, DC> qv;
-        load_query<S, DC>(qv, a.queries + (uint64_t)q * a.D, a.D, lane, a.center, a.u8_inv);
+        load_query<S, DC>(qv, a.queries + (uint64_t)q * a.D, a.D, lane, a.center);
         if constexpr (S::kPQ)
             build_pq_lut<DC>(qv, reinterpret_cast<uint16_t*>(base + lay.lut), a.pq_cb, a.pq_cnorm,
                              a.queries + (uint64_t)q * a.D, a.D, lane);
@@ -461,7 +461,7 @@ __global__ void __launch_bounds__(128, MINB) search_kernel_rw(SearchArgs a) {
                     if (e < a.k) {
                         uint64_t o   = (uint64_t)q * a.k + e;
                         a.out_ids[o] = e < n && e < kq ? (wp[r] & ~kVisitedBit) : kNone;
-                        a.out_d[o]   = e < n && e < kq ? key_dist(wk[r]) * a.out_scale : __int_as_float(0x7f800000);
+                        a.out_d[o]   = e < n && e < kq ? key_dist(wk[r]) : __int_as_float(0x7f800000);
                     }
                 }
             }

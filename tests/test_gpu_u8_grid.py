@@ -128,3 +128,41 @@ def test_integer_rows_keep_the_identity_grid(oracle, vann_mod):
     assert st == 0
     assert np.array_equal(ids.cpu().numpy().view(np.uint32), oids)
     assert np.array_equal(d.cpu().numpy(), od)
+
+
+def test_fitted_grid_rerank_takes_the_best_of_each_list(vann_mod):
+    """With rerank, each query's k results are the k closest (exact distances) of the
+    list the traversal ends with, in order; uneven per-query L and k give what separate
+    searches give."""
+    import torch
+
+    base, q = _fixture(n=8000, seed=89)
+    n, D = base.shape
+    idx = vann_mod.Index(D, 32, 48, 1.2, capacity=n, stores=("f32", "u8"))
+    idx.build(torch.from_numpy(base).cuda(), batch=4000, seed=8)
+    qd = torch.from_numpy(q).cuda()
+    L, k = 40, 10
+    lists, _ = idx.search(qd, k=L, L=L, store="u8", rerank=False)
+    ids, d = idx.search(qd, k=k, L=L, store="u8", rerank=True)
+    lists = lists.cpu().numpy().view(np.uint32).astype(np.int64)
+    ids = ids.cpu().numpy().view(np.uint32).astype(np.int64)
+    d = d.cpu().numpy()
+    for i in range(q.shape[0]):
+        c = lists[i][lists[i] != 0xFFFFFFFF]
+        ex = ((base[c].astype(np.float64) - q[i].astype(np.float64)) ** 2).sum(-1)
+        order = np.argsort(ex, kind="stable")[:k]
+        assert set(ids[i].tolist()) <= set(c.tolist())
+        # the same k rows, in exact-distance order (FP32 sums may swap near-ties only)
+        assert np.allclose(np.sort(ex[order]), np.sort(((base[ids[i]].astype(np.float64) -
+                                                         q[i].astype(np.float64)) ** 2).sum(-1)), rtol=1e-6)
+        assert (np.diff(d[i]) >= 0).all()
+    # uneven: two groups of (L, k) in one launch equal the two separate searches
+    Lq = torch.tensor([32 if i % 2 else 48 for i in range(q.shape[0])], dtype=torch.int32, device="cuda")
+    kq = torch.tensor([5 if i % 2 else 10 for i in range(q.shape[0])], dtype=torch.int32, device="cuda")
+    ui, ud = idx.search_uneven(qd, Lq, kq, store="u8", rerank=True)
+    ui, ud = ui.cpu().numpy(), ud.cpu().numpy()
+    for Lg, kg, sel in ((48, 10, slice(0, None, 2)), (32, 5, slice(1, None, 2))):
+        si, sd = idx.search(qd[sel].contiguous(), k=kg, L=Lg, store="u8", rerank=True)
+        assert np.array_equal(ui[sel][:, :kg], si.cpu().numpy())
+        assert np.array_equal(ud[sel][:, :kg], sd.cpu().numpy())
+        assert (ui[sel][:, kg:] == -1).all()
