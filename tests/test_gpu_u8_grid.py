@@ -47,11 +47,12 @@ def _fixture(n=6000, D=96, seed=81):
     return base, q
 
 
-def test_fitted_grid_traversal_distances_bit_exact(vann_mod):
+@pytest.mark.parametrize("D", [48, 96, 256])
+def test_fitted_grid_traversal_distances_bit_exact(vann_mod, D):
     import torch
 
-    base, q = _fixture()
-    n, D = base.shape
+    base, q = _fixture(D=D)
+    n = base.shape[0]
     idx = vann_mod.Index(D, 32, 48, 1.2, capacity=n, stores=("f32", "u8"))
     idx.build(torch.from_numpy(base).cuda(), batch=2000, seed=5)
     assert idx.info()["entry"] < n
@@ -130,14 +131,15 @@ def test_integer_rows_keep_the_identity_grid(oracle, vann_mod):
     assert np.array_equal(d.cpu().numpy(), od)
 
 
-def test_fitted_grid_rerank_takes_the_best_of_each_list(vann_mod):
+@pytest.mark.parametrize("D", [96, 384])
+def test_fitted_grid_rerank_takes_the_best_of_each_list(vann_mod, D):
     """With rerank, each query's k results are the k closest (exact distances) of the
     list the traversal ends with, in order; uneven per-query L and k give what separate
     searches give."""
     import torch
 
-    base, q = _fixture(n=8000, seed=89)
-    n, D = base.shape
+    base, q = _fixture(n=8000, D=D, seed=89)
+    n = base.shape[0]
     idx = vann_mod.Index(D, 32, 48, 1.2, capacity=n, stores=("f32", "u8"))
     idx.build(torch.from_numpy(base).cuda(), batch=4000, seed=8)
     qd = torch.from_numpy(q).cuda()
