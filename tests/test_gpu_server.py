@@ -173,3 +173,31 @@ def test_large_batches_in_flight_together(vann_mod):
     st = srv.stats()
     assert st["max_inflight"] >= 2, st  # batches overlapped on the device
     srv.close()
+
+
+def test_server_float_rows_on_the_uint8_grid(vann_mod):
+    """Searches served from the uint8 copy of float rows (scalar quantization on the fitted
+    grid, exact FP32 rerank), batched together with uneven k and L, equal the same
+    searches run alone."""
+    import torch
+
+    D = 96
+    base = workload.mixture(6000, D, 30, seed=91, sigma=0.05, integer=False, unit_norm=True)
+    idx = vann_mod.Index(D, 32, 64, 1.2, capacity=len(base), stores=("f32", "u8"))
+    idx.build(torch.from_numpy(base).cuda(), batch=0, seed=14)
+    srv = vann_mod.Server(idx, max_batch=128, slots=3, max_k=32, store="u8", rerank=True)
+    rng = np.random.default_rng(9)
+    ops = []
+    for i in range(120):
+        k = int(rng.choice([1, 10, 32]))
+        L = max(k, int(rng.integers(16, 129)))
+        ops.append((workload.mixture(int(rng.integers(1, 6)), D, 30, seed=30_000 + i, sigma=0.05, integer=False,
+                                     unit_norm=True), k, L))
+    tickets = [srv.submit_search(q, k, L) for q, k, L in ops]
+    results = [srv.wait(t) for t in tickets]
+    assert srv.stats()["batches"] < len(ops)
+    srv.close()
+    for (q, k, L), (ids, d, _) in zip(ops, results):
+        gi, gd = idx.search(torch.from_numpy(q).cuda(), k=k, L=L, store="u8", rerank=True)
+        assert np.array_equal(ids, gi.cpu().numpy().view(np.uint32))
+        assert np.array_equal(d, gd.cpu().numpy())
