@@ -11,7 +11,9 @@
 //   1. candidate ids (A then B, as in prune.cu) with their distances to the node
 //      (given by the search, or computed exactly from the uint8 rows);
 //   2. stable order by (distance, candidate index): each key's rank is the count
-//      of smaller keys (one pass, one barrier);
+//      of smaller keys (in the 256-candidate pass: each warp sorts 64 keys in
+//      registers, then counts the smaller keys of the other three runs by binary
+//      search);
 //   3. the first `cap` candidates' uint8 rows are staged in shared memory in that
 //      order, in the K-major no-swizzle layout tcgen05.mma reads (8-row x 16-byte
 //      core matrices), and one thread issues tcgen05.mma.kind::i8 (u8 x u8 -> s32)
@@ -286,7 +288,40 @@ __global__ void __launch_bounds__(kThreads) prune_tc_kernel(PruneArgs a, uint32_
         __syncthreads();
 
         // --- 3. stable order by (distance, candidate index): rank = keys below
-        {
+        if constexpr (MAXC == 256) {
+            // each warp sorts its 64 keys in registers; a key's rank is then its place in
+            // its own run plus, in each other run, the count of smaller keys (keys are
+            // unique: the candidate index breaks ties)
+            const uint32_t base = 64u * warp;
+            uint64_t       kk[2];
+            kk[0] = base + lane < nc ? keys[base + lane] : ~0ull;
+            kk[1] = base + 32u + lane < nc ? keys[base + 32u + lane] : ~0ull;
+            warp_bitonic_sort<2>(kk, lane, 64u);
+            __syncwarp();  // this warp's keys are read: its run overwrites them
+            keys[base + lane]       = kk[0];
+            keys[base + 32u + lane] = kk[1];
+            __syncthreads();
+#pragma unroll
+            for (uint32_t s2 = 0; s2 < 2; ++s2) {
+                const uint64_t v = kk[s2];
+                if (v == ~0ull) continue;
+                uint32_t r = 32u * s2 + lane;
+                for (uint32_t w2 = 0; w2 < 4; ++w2) {
+                    if (w2 == warp) continue;
+                    const uint64_t* run = keys + 64u * w2;
+                    uint32_t        lo = 0, hi = 64;
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (run[mid] < v)
+                            lo = mid + 1;
+                        else
+                            hi = mid;
+                    }
+                    r += lo;
+                }
+                perm[r] = (uint32_t)v;
+            }
+        } else {
             uint64_t k[KPT];
             uint32_t r[KPT];
 #pragma unroll
@@ -359,13 +394,24 @@ __global__ void __launch_bounds__(kThreads) prune_tc_kernel(PruneArgs a, uint32_
                 n = dp4a_u(v.x, v.x, dp4a_u(v.y, v.y, dp4a_u(v.z, v.z, dp4a_u(v.w, v.w, n))));
             }
             nrm[t] = n;
+            // "t prunes u" is alpha * d(t, u) <= d(node, u) in FP32, with d(t, u) the exact
+            // integer Y = |t|^2 + |u|^2 - 2 t.u (< 2^24, so FP32 holds it exactly).  fl(Y *
+            // alpha) does not decrease as Y grows, so the test is Y <= Ymax(u), the largest
+            // integer with fl(Ymax * alpha) <= d(node, u): 2 t.u - |t|^2 >= |u|^2 - Ymax(u).
+            // That threshold replaces d(node, u) in the same slot.
+            const float sdt = sd[t];
+            int         y   = (int)fminf(floorf(sdt / a.alpha), 16777215.f);
+            while (y < 16777215 && (float)(y + 1) * a.alpha <= sdt) ++y;
+            while (y > 0 && (float)y * a.alpha > sdt) --y;
+            reinterpret_cast<int*>(sd)[t] = (int)n - y;
         }
         __syncthreads();
+        const int* thr = reinterpret_cast<const int*>(sd);
 
         // --- 6. prune masks in sorted order: bit u of row t = "t, once chosen, prunes u"
         for (uint32_t r = 0; r < nb; ++r) {
             const uint32_t t  = 128u * r + tid;
-            const uint32_t nt = t < m ? nrm[t] : 0u;
+            const int      nt = t < m ? (int)nrm[t] : 0;
             uint32_t       mk[QW];
 #pragma unroll
             for (uint32_t q = 0; q < QW; ++q) mk[q] = 0u;
@@ -398,8 +444,7 @@ __global__ void __launch_bounds__(kThreads) prune_tc_kernel(PruneArgs a, uint32_
 #pragma unroll
                             for (uint32_t k = 0; k < 16; ++k) {
                                 const uint32_t u = 128u * c + c16 + k;
-                                const float    y = (float)(nt + nrm[u] - 2u * g[k]);
-                                bits |= (uint32_t)(y * a.alpha <= sd[u]) << k;
+                                bits |= (uint32_t)((int)(2u * g[k]) - nt >= thr[u]) << k;
                             }
                             mk[4u * c + (c16 >> 5)] |= bits << (c16 & 16u);
                         }
