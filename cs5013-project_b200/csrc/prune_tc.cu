@@ -11,9 +11,7 @@
 //   1. candidate ids (A then B, as in prune.cu) with their distances to the node
 //      (given by the search, or computed exactly from the uint8 rows);
 //   2. stable order by (distance, candidate index): each key's rank is the count
-//      of smaller keys (in the 256-candidate pass: each warp sorts 64 keys in
-//      registers, then counts the smaller keys of the other three runs by binary
-//      search);
+//      of smaller keys (one pass, one barrier);
 //   3. the first `cap` candidates' uint8 rows are staged in shared memory in that
 //      order, in the K-major no-swizzle layout tcgen05.mma reads (8-row x 16-byte
 //      core matrices), and one thread issues tcgen05.mma.kind::i8 (u8 x u8 -> s32)
@@ -288,40 +286,7 @@ __global__ void __launch_bounds__(kThreads) prune_tc_kernel(PruneArgs a, uint32_
         __syncthreads();
 
         // --- 3. stable order by (distance, candidate index): rank = keys below
-        if constexpr (MAXC == 256) {
-            // each warp sorts its 64 keys in registers; a key's rank is then its place in
-            // its own run plus, in each other run, the count of smaller keys (keys are
-            // unique: the candidate index breaks ties)
-            const uint32_t base = 64u * warp;
-            uint64_t       kk[2];
-            kk[0] = base + lane < nc ? keys[base + lane] : ~0ull;
-            kk[1] = base + 32u + lane < nc ? keys[base + 32u + lane] : ~0ull;
-            warp_bitonic_sort<2>(kk, lane, 64u);
-            __syncwarp();  // this warp's keys are read: its run overwrites them
-            keys[base + lane]       = kk[0];
-            keys[base + 32u + lane] = kk[1];
-            __syncthreads();
-#pragma unroll
-            for (uint32_t s2 = 0; s2 < 2; ++s2) {
-                const uint64_t v = kk[s2];
-                if (v == ~0ull) continue;
-                uint32_t r = 32u * s2 + lane;
-                for (uint32_t w2 = 0; w2 < 4; ++w2) {
-                    if (w2 == warp) continue;
-                    const uint64_t* run = keys + 64u * w2;
-                    uint32_t        lo = 0, hi = 64;
-                    while (lo < hi) {
-                        const uint32_t mid = (lo + hi) >> 1;
-                        if (run[mid] < v)
-                            lo = mid + 1;
-                        else
-                            hi = mid;
-                    }
-                    r += lo;
-                }
-                perm[r] = (uint32_t)v;
-            }
-        } else {
+        {
             uint64_t k[KPT];
             uint32_t r[KPT];
 #pragma unroll
