@@ -168,3 +168,31 @@ def test_fitted_grid_rerank_takes_the_best_of_each_list(vann_mod, D):
         assert np.array_equal(ui[sel][:, :kg], si.cpu().numpy())
         assert np.array_equal(ud[sel][:, :kg], sd.cpu().numpy())
         assert (ui[sel][:, kg:] == -1).all()
+
+
+@pytest.mark.parametrize("L", [32, 64, 100])
+def test_fitted_grid_search_is_the_oracle_search_on_the_codes(oracle, vann_mod, L):
+    """On its fitted grid the uint8 search is the reference's GreedySearch over the code
+    rows with the rounded queries: the oracle, given the codes as its rows, returns the
+    same ids, hops and distance evaluations, and its (exact integer) distances times s^2
+    are the returned distances, bit for bit; L = 100 takes the shared-memory worklist."""
+    import torch
+
+    base, q = _fixture(n=6000, seed=93)
+    n, D = base.shape
+    idx = vann_mod.Index(D, 32, 64, 1.2, capacity=n, stores=("f32", "u8"))
+    idx.build(torch.from_numpy(base).cuda(), batch=2000, seed=9)
+    _, deg, adj = idx.get_graph()
+    entry = idx.info()["entry"]
+    lo, s, inv = _grid(base)
+    codes = _codes(base, lo, inv).astype(np.float32)
+    qcodes = _codes(q, lo, inv).astype(np.float32)
+    g = oracle.Graph(codes, deg, adj)
+    st, oids, od, ohops, oevals = g.search(qcodes, L, 10, entry, bloom_mode=oracle.BLOOM_SNAPSHOT)
+    assert st == 0
+    ids, d, stats = idx.search_stats(torch.from_numpy(q).cuda(), k=10, L=L, store="u8", rerank=False)
+    assert np.array_equal(ids.cpu().numpy().view(np.uint32), oids)
+    s2 = np.float32(s) * np.float32(s)
+    assert np.array_equal(d.cpu().numpy(), od.astype(np.float32) * s2)
+    stats = stats.cpu().numpy()
+    assert np.array_equal(stats[0], ohops) and np.array_equal(stats[1].astype(np.int64), oevals)
