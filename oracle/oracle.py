@@ -75,6 +75,11 @@ def lib():
         L.vo_bruteforce_knn.restype = None
         L.vo_bruteforce_knn.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, C.c_int,
                                         C.c_void_p, C.c_void_p, C.c_int]
+        L.vo_u8_grid.restype = C.c_int
+        L.vo_u8_grid.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.POINTER(C.c_float),
+                                 C.POINTER(C.c_float)]
+        L.vo_u8_codes.restype = None
+        L.vo_u8_codes.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_float, C.c_void_p]
         L.vo_merge_rerank.restype = None
         L.vo_merge_rerank.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_int,
                                       C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
@@ -252,3 +257,22 @@ def recall_at_k(found: np.ndarray, truth: np.ndarray, k: int) -> float:
     for f, t in zip(found[:, :k], truth[:, :k]):
         hit += len(set(f.tolist()) & set(t.tolist()))
     return hit / (truth.shape[0] * k)
+
+
+def u8_grid(vecs: np.ndarray):
+    """The uint8 copy's grid fitted to `vecs` (vo_u8_grid): (fitted, lo[dim], s, inv);
+    fitted False means the identity grid (every value an integer in [0, 255])."""
+    v = np.ascontiguousarray(vecs, dtype=np.float32)
+    lo = np.empty(v.shape[1], np.float32)
+    s, inv = C.c_float(), C.c_float()
+    fitted = lib().vo_u8_grid(_p(v), v.shape[0], v.shape[1], _p(lo), C.byref(s), C.byref(inv))
+    return bool(fitted), lo, np.float32(s.value), np.float32(inv.value)
+
+
+def u8_codes(x: np.ndarray, lo, inv) -> np.ndarray:
+    """Codes of rows or queries on a grid (vo_u8_codes); lo None: the identity grid."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty(x.shape, np.uint8)
+    lo_c = None if lo is None else np.ascontiguousarray(lo, dtype=np.float32)
+    lib().vo_u8_codes(_p(x), x.shape[0], x.shape[1], _p(lo_c), float(inv), _p(out))
+    return out

@@ -710,3 +710,48 @@ int vo_consolidate(vo_graph* g, float alpha, int cap, const unsigned char* is_fr
     if (new_entry) *new_entry = ne;
     return VO_OK;
 }
+
+/* ---------------------------------------------------------------- uint8 grid */
+/* The product's uint8 copy of float rows (cs5013-project_b200/csrc/graph_ops.cu
+ * launch_u8_grid, convert_kernel; queries: csrc/rerank.cu grid_queries_kernel),
+ * restated so the tests check its codes and its search against the oracle. */
+int vo_u8_grid(const float* vecs, int64_t n, int dim, float* lo, float* s, float* inv) {
+    int    affine = 0;
+    float* hi     = (float*)malloc(sizeof(float) * (size_t)dim);
+    for (int d = 0; d < dim; ++d) {
+        lo[d] = INFINITY;
+        hi[d] = -INFINITY;
+    }
+    for (int64_t i = 0; i < n; ++i)
+        for (int d = 0; d < dim; ++d) {
+            const float x = vecs[(size_t)i * dim + d];
+            if (x < lo[d]) lo[d] = x;
+            if (x > hi[d]) hi[d] = x;
+            if (!(x >= 0.f && x <= 255.f && rintf(x) == x)) affine = 1;
+        }
+    float range = 0.f;
+    for (int d = 0; d < dim; ++d) {
+        const float r = hi[d] - lo[d];
+        if (r > range) range = r;
+    }
+    free(hi);
+    if (!affine) {
+        for (int d = 0; d < dim; ++d) lo[d] = 0.f;
+        *s   = 1.f;
+        *inv = 1.f;
+        return 0;
+    }
+    *s   = range > 0.f ? range / 255.f : 1.f;
+    *inv = 1.f / *s;
+    return 1;
+}
+
+void vo_u8_codes(const float* x, int64_t n, int dim, const float* lo, float inv, uint8_t* out) {
+    for (int64_t i = 0; i < n; ++i)
+        for (int d = 0; d < dim; ++d) {
+            const float v = x[(size_t)i * dim + d];
+            float       c = lo ? rintf((v - lo[d]) * inv) : rintf(v);
+            c             = c < 0.f ? 0.f : (c > 255.f ? 255.f : c);
+            out[(size_t)i * dim + d] = (uint8_t)c;
+        }
+}

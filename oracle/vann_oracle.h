@@ -120,6 +120,16 @@ void vo_merge_rerank(const float* vecs, int dim, const float* q, int64_t nq, con
 void vo_bruteforce_knn(const float* base, int64_t n, const float* q, int64_t nq, int dim, int k,
                        uint32_t* out_ids, double* out_d, int threads);
 
+/* The uint8 traversal copy of float rows (no counterpart in the reference: a
+ * reduced-precision form beside it).  The grid fitted to rows 0 .. n-1: when every
+ * value is an integer in [0, 255] the identity (returns 0; lo = 0, s = inv = 1), else
+ * (returns 1) lo[d] = the column minimum and one scale s = max_d (max_d - lo[d]) / 255
+ * (1 when every column is constant), inv = 1 / s, all in FP32. */
+int vo_u8_grid(const float* vecs, int64_t n, int dim, float* lo, float* s, float* inv);
+/* Codes of n rows (or queries) on a grid: rint((x - lo[d]) * inv) clamped to [0, 255]
+ * (round half to even); lo NULL: the identity grid, rint(x) clamped. */
+void vo_u8_codes(const float* x, int64_t n, int dim, const float* lo, float inv, uint8_t* out);
+
 #ifdef __cplusplus
 }
 #endif

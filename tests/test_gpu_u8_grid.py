@@ -5,7 +5,8 @@ Rows that are not all integers in [0, 255] get a grid with one offset per dimens
 Codes are round((x - lo) / s), clamped to [0, 255]; a query is mapped onto the same
 grid and rounded, and the search runs the exact dp4a path on the codes.  Returned
 traversal distances are the code distances times s^2, so they are restated here bit
-for bit in numpy (FP32 arithmetic, as the kernels do it).  With rerank the returned
+for bit from the oracle's restatement of the grid (vo_u8_grid, vo_u8_codes: FP32
+arithmetic, as the kernels do it).  With rerank the returned
 distances are exact FP32 and recall matches the FP32 form's.
 """
 import numpy as np
@@ -16,23 +17,22 @@ from vann import workload
 pytestmark = pytest.mark.gpu
 
 
-def _grid(rows):
-    """The grid the library fits to `rows`: offsets, scale, 1 / scale (all FP32)."""
-    rows = rows.astype(np.float32)
-    lo = rows.min(0)
-    rng = (rows.max(0) - lo).max()
-    s = np.float32(rng) / np.float32(255.0) if rng > 0 else np.float32(1.0)
-    return lo, np.float32(s), np.float32(1.0) / np.float32(s)
+def _grid(oracle, rows):
+    """The grid the library fits to `rows` (the oracle's vo_u8_grid): offsets, scale,
+    1 / scale, all FP32; these rows are float, so the grid is a fitted one."""
+    fitted, lo, s, inv = oracle.u8_grid(rows)
+    assert fitted
+    return lo, s, inv
 
 
-def _codes(x, lo, inv):
-    return np.clip(np.rint((x.astype(np.float32) - lo) * inv), 0, 255).astype(np.int64)
+def _codes(oracle, x, lo, inv):
+    return oracle.u8_codes(x, lo, inv).astype(np.int64)
 
 
-def _code_dists(q, base, ids, lo, s, inv):
+def _code_dists(oracle, q, base, ids, lo, s, inv):
     """s^2 * squared code distance of every returned id, as the kernel forms it."""
-    qc = _codes(q, lo, inv)
-    bc = _codes(base, lo, inv)
+    qc = _codes(oracle, q, lo, inv)
+    bc = _codes(oracle, base, lo, inv)
     out = np.empty(ids.shape, np.float32)
     s2 = np.float32(s) * np.float32(s)
     for i in range(ids.shape[0]):
@@ -48,7 +48,7 @@ def _fixture(n=6000, D=96, seed=81):
 
 
 @pytest.mark.parametrize("D", [48, 96, 256])
-def test_fitted_grid_traversal_distances_bit_exact(vann_mod, D):
+def test_fitted_grid_traversal_distances_bit_exact(oracle, vann_mod, D):
     import torch
 
     base, q = _fixture(D=D)
@@ -56,14 +56,14 @@ def test_fitted_grid_traversal_distances_bit_exact(vann_mod, D):
     idx = vann_mod.Index(D, 32, 48, 1.2, capacity=n, stores=("f32", "u8"))
     idx.build(torch.from_numpy(base).cuda(), batch=2000, seed=5)
     assert idx.info()["entry"] < n
-    lo, s, inv = _grid(base)
+    lo, s, inv = _grid(oracle, base)
     qd = torch.from_numpy(q).cuda()
     for L in (32, 48):
         ids, d = idx.search(qd, k=10, L=L, store="u8", rerank=False)
         gi = ids.cpu().numpy().view(np.uint32)
         gd = d.cpu().numpy()
         assert (gi < n).all()
-        assert np.array_equal(gd, _code_dists(q, base, gi.astype(np.int64), lo, s, inv))
+        assert np.array_equal(gd, _code_dists(oracle, q, base, gi.astype(np.int64), lo, s, inv))
         assert (np.diff(gd, axis=1) >= 0).all()
 
 
@@ -93,7 +93,7 @@ def test_fitted_grid_rerank_recall_and_exact_distances(oracle, vann_mod):
     assert rel.mean() < 8e-3 and rel.max() < 0.05, (rel.mean(), rel.max())
 
 
-def test_grid_fixed_for_later_inserts(vann_mod):
+def test_grid_fixed_for_later_inserts(oracle, vann_mod):
     """Rows inserted after the build are coded on the build's grid (no refit), values
     beyond its range clamped to the end codes."""
     import torch
@@ -108,10 +108,10 @@ def test_grid_fixed_for_later_inserts(vann_mod):
     idx.build(torch.from_numpy(rows[:first]).cuda(), batch=0, seed=7)
     idx.insert(torch.from_numpy(rows[first:]).cuda())
     idx.sync()
-    lo, s, inv = _grid(rows[:first])
+    lo, s, inv = _grid(oracle, rows[:first])
     ids, d = idx.search(torch.from_numpy(q).cuda(), k=10, L=48, store="u8", rerank=False)
     gi = ids.cpu().numpy().view(np.uint32).astype(np.int64)
-    assert np.array_equal(d.cpu().numpy(), _code_dists(q, rows, gi, lo, s, inv))
+    assert np.array_equal(d.cpu().numpy(), _code_dists(oracle, q, rows, gi, lo, s, inv))
     assert (gi >= first).any()  # inserted rows are found
 
 
@@ -184,9 +184,9 @@ def test_fitted_grid_search_is_the_oracle_search_on_the_codes(oracle, vann_mod, 
     idx.build(torch.from_numpy(base).cuda(), batch=2000, seed=9)
     _, deg, adj = idx.get_graph()
     entry = idx.info()["entry"]
-    lo, s, inv = _grid(base)
-    codes = _codes(base, lo, inv).astype(np.float32)
-    qcodes = _codes(q, lo, inv).astype(np.float32)
+    lo, s, inv = _grid(oracle, base)
+    codes = _codes(oracle, base, lo, inv).astype(np.float32)
+    qcodes = _codes(oracle, q, lo, inv).astype(np.float32)
     g = oracle.Graph(codes, deg, adj)
     st, oids, od, ohops, oevals = g.search(qcodes, L, 10, entry, bloom_mode=oracle.BLOOM_SNAPSHOT)
     assert st == 0
