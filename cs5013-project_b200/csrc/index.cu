@@ -1098,6 +1098,28 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
         a.adjw_out = d_adjw;
         a.Lq = h->pending_Lq;
         a.kq = h->pending_kq;
+        // a search over the uint8 copy on a fitted grid needs a per-stream workspace (the
+        // queries on the grid, and with rerank the candidate lists): sized here, before
+        // anything is queued, and never allocated while the stream is being captured
+        DevBuf* grid_ws = nullptr;
+        if (sp->store == VANN_STORE_U8 && h->u8_affine) {
+            const size_t need = sizeof(float) * nq * h->p.dim +
+                                (sp->rerank ? (sizeof(uint32_t) + sizeof(float)) * nq * sp->L : 0);
+            grid_ws = &h->grid_ws[S(stream)];
+            if (grid_ws->bytes < need) {
+                cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+                VCHECK(cudaStreamIsCapturing(S(stream), &cs));
+                VREQUIRE(cs == cudaStreamCaptureStatusNone, VANN_ERR_STATE,
+                         "a search over the fitted uint8 grid needs its workspace before capture: run one "
+                         "search of this size on the stream first");
+                if (grid_ws->p) {  // a captured search may hold the old one: keep it until destroy
+                    h->ord_retired.push_back(grid_ws->p);
+                    grid_ws->p     = nullptr;
+                    grid_ws->bytes = 0;
+                }
+                grid_ws->ensure(need);
+            }
+        }
         // the order kernel zeroes the counter, else a memset does
         a.counter  = h->next_counter(S(stream), false);
         bool chain = false;
@@ -1105,29 +1127,15 @@ vann_status vann_search_stats(vann_index* h, const float* d_queries, uint64_t nq
         if (a.order == nullptr) VCHECK(cudaMemsetAsync(a.counter, 0, sizeof(uint32_t), S(stream)));
         a.pdl = chain ? 1 : 0;
         a.status = h->status;
-        if (sp->store == VANN_STORE_U8 && h->u8_affine) {
+        if (grid_ws != nullptr) {
             // uint8 copy on a fitted grid: the queries rounded onto the grid, the search on
             // code distances, then the exact FP32 rerank of each list, or the distances
             // scaled back by s^2 (the queries' order above comes from the FP32 queries)
             cudaStream_t   st   = S(stream);
             const uint32_t L    = sp->L;
             const size_t   qb   = sizeof(float) * nq * h->p.dim;
-            const size_t   cb   = sp->rerank ? (sizeof(uint32_t) + sizeof(float)) * nq * L : 0;
-            DevBuf&        ws   = h->grid_ws[st];
-            if (ws.bytes < qb + cb) {
-                cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-                VCHECK(cudaStreamIsCapturing(st, &cs));
-                VREQUIRE(cs == cudaStreamCaptureStatusNone, VANN_ERR_STATE,
-                         "a search over the fitted uint8 grid needs its workspace before capture: run one "
-                         "search of this size on the stream first");
-                if (ws.p) {  // a captured search may hold the old one: keep it until destroy
-                    h->ord_retired.push_back(ws.p);
-                    ws.p     = nullptr;
-                    ws.bytes = 0;
-                }
-                ws.ensure(qb + cb);
-            }
-            float* qg = ws.as<float>();
+            DevBuf&        ws   = *grid_ws;
+            float*         qg   = ws.as<float>();
             VCHECK(vann::launch_grid_queries(d_queries, nq, h->p.dim, h->u8_lo, h->u8_inv, qg, st));
             a.queries = qg;
             a.rerank  = 0;
